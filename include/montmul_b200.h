@@ -1,0 +1,108 @@
+/* montmul_b200 — C ABI of the B200 backend for MontMul's batched Montgomery step
+ * x <- x^2 c R^-1 mod N (and a b R^-1 mod N) over many independent odd moduli.
+ *
+ * The ABI mirrors the reference's backend contract, the `Limits` and `Backend` traits of
+ * montmul/src/transform.rs:11-20 and 61-77, as implemented by the CUDA backend `Gpu`
+ * (montmul/src/gpu/mod.rs:321-398). The caller (the host API `ModBatch`, batch.rs:130-261)
+ * keeps the big-integer work — N' = -N^-1 mod R, Montgomery conversion, is_one — and passes
+ * plain little-endian 32-bit limb arrays.
+ *
+ * Conventions (the reference panics where this ABI returns a status):
+ *   - every call that can fail returns an int status (MM_OK = 0); mm_b200_last_error() then
+ *     describes it with the reference's wording ("batch needs ... bytes", "carry out of a
+ *     product that must fit, slot i");
+ *   - the backend copies every input; the caller owns its buffers;
+ *   - one batch is used by one host thread at a time (the trait's &mut State).
+ * The wraparound path is always on (k = L/2, GpuOptions::wraparound, gpu/mod.rs:36-44).
+ */
+#ifndef MONTMUL_B200_H
+#define MONTMUL_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    MM_OK = 0,
+    MM_ERR_ARG = 1,          /* bad argument (index, size, unsupported length, ...) */
+    MM_ERR_OOM = 2,          /* batch does not fit in device memory (message names the bytes) */
+    MM_ERR_CARRY = 3,        /* a carry that must vanish did not (message names the slot) */
+    MM_ERR_CUDA = 4,         /* CUDA runtime error (message carries the runtime's text) */
+    MM_ERR_UNSUPPORTED = 5   /* a configuration this build does not run */
+};
+
+typedef struct mm_b200_device mm_b200_device; /* `Gpu` (gpu/mod.rs:47-54): one CUDA device */
+typedef struct mm_b200_batch mm_b200_batch;   /* `GpuState` (gpu/mod.rs:237-258): one batch */
+
+/* `GpuOptions` (gpu/mod.rs:28-45). max_launch_steps bounds the steps of one kernel launch
+ * (the reference bounds launches by time, max_launch_ms); 0 selects the default. */
+typedef struct {
+    int device;
+    int force_global;
+    int wraparound;
+    int max_launch_steps;
+} mm_b200_options;
+
+/* Message of the last failing call on this host thread ("" if none). */
+const char *mm_b200_last_error(void);
+
+/* Gpu::with_options (gpu/mod.rs:62-67). */
+int mm_b200_open(const mm_b200_options *opts, mm_b200_device **out);
+void mm_b200_close(mm_b200_device *dev);
+/* Gpu::sm_count / free_memory / max_dyn_smem / device_name (gpu/mod.rs:83-99). */
+int mm_b200_sm_count(const mm_b200_device *dev);
+size_t mm_b200_free_memory(mm_b200_device *dev);
+int mm_b200_max_dyn_smem(const mm_b200_device *dev);
+const char *mm_b200_device_name(const mm_b200_device *dev);
+
+/* Limits (transform.rs:11-20): Q = M31 * M61 as two 64-bit halves (lo, hi); the supported
+ * transform lengths L ascending (returns their number, writes at most cap); full_k. */
+void mm_b200_coefficient_bound(uint64_t out[2]);
+size_t mm_b200_supported_lengths(size_t *out, size_t cap);
+int mm_b200_full_k(const mm_b200_device *dev);
+
+/* Device bytes a batch of `slots` slots at length `len` takes (Gpu::create's check,
+ * gpu/mod.rs:332, with this backend's buffers). */
+size_t mm_b200_batch_bytes(size_t slots, size_t len, size_t exp_words);
+
+/* Backend::create (transform.rs:64; gpu/mod.rs:325-370). n, nprime, two_n: slots x k limbs,
+ * row-major (BatchSetup, transform.rs:49-59). k must equal len / 2. */
+int mm_b200_create(mm_b200_device *dev, size_t k, size_t len, uint32_t base, size_t slots,
+                   const uint32_t *n, const uint32_t *nprime, const uint32_t *two_n,
+                   mm_b200_batch **out);
+/* Backend::load (transform.rs:65-66): k limbs of a Montgomery-form value in [0, 2N). */
+int mm_b200_load(mm_b200_batch *b, size_t i, const uint32_t *limbs);
+/* All slots at once: slots x k limbs. */
+int mm_b200_load_all(mm_b200_batch *b, const uint32_t *limbs);
+/* Backend::set_exponent (transform.rs:67-68): MSB-first words; resets the slot's position. */
+int mm_b200_set_exponent(mm_b200_batch *b, size_t i, const uint32_t *words, size_t nwords, size_t nbits);
+/* All slots at once: slots x ew words and slots bit counts. */
+int mm_b200_set_exponents(mm_b200_batch *b, const uint32_t *words, size_t ew, const uint32_t *nbits);
+/* Backend::run (transform.rs:69-70): up to `bits` steps on every slot with bits left. */
+int mm_b200_run(mm_b200_batch *b, size_t bits);
+/* Backend::mul (transform.rs:71-72): slot out <- a b R^-1, slots sharing a modulus. */
+int mm_b200_mul(mm_b200_batch *b, size_t out, size_t a, size_t bb);
+/* Backend::read (transform.rs:73-74): k limbs in [0, 2N). */
+int mm_b200_read(mm_b200_batch *b, size_t i, uint32_t *limbs);
+int mm_b200_read_all(mm_b200_batch *b, uint32_t *limbs);
+/* Backend::remaining (transform.rs:75-76). */
+size_t mm_b200_remaining(const mm_b200_batch *b, size_t i);
+size_t mm_b200_slots(const mm_b200_batch *b);
+void mm_b200_destroy(mm_b200_batch *b);
+
+/* Asynchronous form of run for timing: enqueues the launches on the batch's stream and
+ * returns; mm_b200_sync waits and performs run's error check. mm_b200_stream is the
+ * cudaStream_t the batch launches on. */
+int mm_b200_run_async(mm_b200_batch *b, size_t bits);
+int mm_b200_sync(mm_b200_batch *b);
+void *mm_b200_stream(mm_b200_batch *b);
+/* Kernel launches issued by this batch so far (for launch accounting). */
+uint64_t mm_b200_launches(const mm_b200_batch *b);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,194 @@
+"""The B200 backend: a ctypes binding of the C ABI in include/montmul_b200.h.
+
+`B200` plays the role of the reference's `Gpu` backend (montmul/src/gpu/mod.rs) behind the
+same `Limits` + `Backend` methods, so `ModBatch(B200(), moduli, 3)` drives the CUDA kernels.
+There is no CPU fallback: constructing a `B200` without the built library or without a CUDA
+device raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from .batch import MontMulError
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libmontmul_b200.so")
+
+MM_OK, MM_ERR_ARG, MM_ERR_OOM, MM_ERR_CARRY, MM_ERR_CUDA, MM_ERR_UNSUPPORTED = range(6)
+
+# Every symbol include/montmul_b200.h declares, with (argtypes, restype).
+_u32p = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
+_sz = C.c_size_t
+_vp = C.c_void_p
+
+
+class Options(C.Structure):
+    """mm_b200_options (GpuOptions, gpu/mod.rs:28-45)."""
+    _fields_ = [("device", C.c_int), ("force_global", C.c_int), ("wraparound", C.c_int),
+                ("max_launch_steps", C.c_int)]
+
+
+SIGNATURES = {
+    "mm_b200_last_error": ([], C.c_char_p),
+    "mm_b200_open": ([C.POINTER(Options), C.POINTER(_vp)], C.c_int),
+    "mm_b200_close": ([_vp], None),
+    "mm_b200_sm_count": ([_vp], C.c_int),
+    "mm_b200_free_memory": ([_vp], _sz),
+    "mm_b200_max_dyn_smem": ([_vp], C.c_int),
+    "mm_b200_device_name": ([_vp], C.c_char_p),
+    "mm_b200_coefficient_bound": ([C.POINTER(C.c_uint64)], None),
+    "mm_b200_supported_lengths": ([C.POINTER(_sz), _sz], _sz),
+    "mm_b200_full_k": ([_vp], C.c_int),
+    "mm_b200_batch_bytes": ([_sz, _sz, _sz], _sz),
+    "mm_b200_create": ([_vp, _sz, _sz, C.c_uint32, _sz, _u32p, _u32p, _u32p, C.POINTER(_vp)], C.c_int),
+    "mm_b200_load": ([_vp, _sz, _u32p], C.c_int),
+    "mm_b200_load_all": ([_vp, _u32p], C.c_int),
+    "mm_b200_set_exponent": ([_vp, _sz, _u32p, _sz, _sz], C.c_int),
+    "mm_b200_set_exponents": ([_vp, _u32p, _sz, _u32p], C.c_int),
+    "mm_b200_run": ([_vp, _sz], C.c_int),
+    "mm_b200_mul": ([_vp, _sz, _sz, _sz], C.c_int),
+    "mm_b200_read": ([_vp, _sz, _u32p], C.c_int),
+    "mm_b200_read_all": ([_vp, _u32p], C.c_int),
+    "mm_b200_remaining": ([_vp, _sz], _sz),
+    "mm_b200_slots": ([_vp], _sz),
+    "mm_b200_destroy": ([_vp], None),
+    "mm_b200_run_async": ([_vp, _sz], C.c_int),
+    "mm_b200_sync": ([_vp], C.c_int),
+    "mm_b200_stream": ([_vp], _vp),
+    "mm_b200_launches": ([_vp], C.c_uint64),
+}
+
+_lib = None
+
+
+def lib():
+    """Loads the in-tree CUDA library; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise MontMulError(f"{LIB_PATH} is missing: build it with `python -m montmul_b200.build`")
+        L = C.CDLL(LIB_PATH)
+        for name, (args, res) in SIGNATURES.items():
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = res
+        _lib = L
+    return _lib
+
+
+def _check(rc: int) -> None:
+    if rc != MM_OK:
+        msg = lib().mm_b200_last_error().decode()
+        raise MontMulError(msg)
+
+
+class _Batch:
+    def __init__(self, ptr, k, slots):
+        self.ptr, self.k, self.slots = ptr, k, slots
+
+    def __del__(self):
+        if self.ptr:
+            lib().mm_b200_destroy(self.ptr)
+            self.ptr = None
+
+
+class B200:
+    """`Gpu`-equivalent backend on one B200 (wraparound path, k = L/2)."""
+
+    def __init__(self, device: int = 0, max_launch_steps: int = 0):
+        opts = Options(device, 0, 1, max_launch_steps)
+        ptr = _vp()
+        _check(lib().mm_b200_open(C.byref(opts), C.byref(ptr)))
+        self._dev = ptr
+        n = lib().mm_b200_supported_lengths(None, 0)
+        arr = (_sz * n)()
+        lib().mm_b200_supported_lengths(arr, n)
+        self._lengths = [int(v) for v in arr]
+
+    def __del__(self):
+        if getattr(self, "_dev", None):
+            lib().mm_b200_close(self._dev)
+            self._dev = None
+
+    # Limits (transform.rs:11-20)
+    def coefficient_bound(self) -> int:
+        q = (C.c_uint64 * 2)()
+        lib().mm_b200_coefficient_bound(q)
+        return int(q[0]) | (int(q[1]) << 64)
+
+    def supported_lengths(self):
+        return list(self._lengths)
+
+    def full_k(self) -> bool:
+        return bool(lib().mm_b200_full_k(self._dev))
+
+    # device facts (gpu/mod.rs:83-99)
+    def sm_count(self) -> int:
+        return int(lib().mm_b200_sm_count(self._dev))
+
+    def free_memory(self) -> int:
+        return int(lib().mm_b200_free_memory(self._dev))
+
+    def device_name(self) -> str:
+        return lib().mm_b200_device_name(self._dev).decode()
+
+    # Backend (transform.rs:61-77)
+    def create(self, k, length, base, n, nprime, two_n):
+        slots = n.shape[0]
+        ptr = _vp()
+        _check(lib().mm_b200_create(self._dev, k, length, base, slots, np.ascontiguousarray(n, np.uint32),
+                                    np.ascontiguousarray(nprime, np.uint32),
+                                    np.ascontiguousarray(two_n, np.uint32), C.byref(ptr)))
+        st = _Batch(ptr, k, slots)
+        st.owner = self   # keep the device open while the batch lives
+        return st
+
+    def load(self, st, i, limbs):
+        _check(lib().mm_b200_load(st.ptr, i, np.ascontiguousarray(limbs, np.uint32)))
+
+    def load_all(self, st, limbs):
+        _check(lib().mm_b200_load_all(st.ptr, np.ascontiguousarray(limbs, np.uint32)))
+
+    def set_exponent(self, st, i, words, nbits):
+        w = np.ascontiguousarray(words, np.uint32)
+        if w.size == 0:
+            w = np.zeros(1, np.uint32)
+        _check(lib().mm_b200_set_exponent(st.ptr, i, w, len(words), nbits))
+
+    def set_exponents(self, st, words, nbits):
+        words = np.ascontiguousarray(words, np.uint32)
+        _check(lib().mm_b200_set_exponents(st.ptr, words, words.shape[1], np.ascontiguousarray(nbits, np.uint32)))
+
+    def run(self, st, bits):
+        _check(lib().mm_b200_run(st.ptr, bits))
+
+    def run_async(self, st, bits):
+        _check(lib().mm_b200_run_async(st.ptr, bits))
+
+    def sync(self, st):
+        _check(lib().mm_b200_sync(st.ptr))
+
+    def stream(self, st) -> int:
+        return int(lib().mm_b200_stream(st.ptr) or 0)
+
+    def launches(self, st) -> int:
+        return int(lib().mm_b200_launches(st.ptr))
+
+    def mul(self, st, out, a, b):
+        _check(lib().mm_b200_mul(st.ptr, out, a, b))
+
+    def read(self, st, i):
+        o = np.zeros(st.k, np.uint32)
+        _check(lib().mm_b200_read(st.ptr, i, o))
+        return o
+
+    def read_all(self, st):
+        o = np.zeros((st.slots, st.k), np.uint32)
+        _check(lib().mm_b200_read_all(st.ptr, o))
+        return o
+
+    def remaining(self, st, i):
+        return int(lib().mm_b200_remaining(st.ptr, i))

@@ -1,0 +1,47 @@
+// Host-visible interface between the backend (mm_backend.cu) and the per-length kernel
+// instantiations (mm_inst.cu, compiled once per log2 n): the kernel argument block and the
+// table of kernel entry points of one length.
+#pragma once
+#include "mm_common.h"
+
+namespace mm {
+
+// Per-batch device state, structure of arrays over slots.
+struct SlotArgs {
+    uint32_t* x;          // slots x k limbs, Montgomery form in [0, 2N)
+    uint32_t* tbuf;       // slots x 2n limbs: T of the step in flight
+    const F2* c2;         // slots x 2n: F(N') in fused-pass order, then A | B
+    const F1* c1;
+    const uint32_t* exp;  // slots x ew words, most significant bit first
+    const uint32_t* nbits;
+    uint32_t* pos;
+    uint32_t* err;        // set to 1 when a carry that must vanish does not
+    const F2* tab2;       // this length's tables (mm_common.h layout)
+    const F1* tab1;
+    uint32_t ew;
+    uint32_t base;
+};
+
+typedef void (*StepFn)(SlotArgs, uint32_t, uint32_t);
+typedef void (*MulFn)(SlotArgs, uint32_t, uint32_t, uint32_t, F2*, F1*);
+typedef void (*SetupFn)(const uint32_t*, const uint32_t*, F2*, F1*, const F2*, const F1*, F2, F1, uint32_t);
+
+struct KernelSet {
+    StepFn step;
+    MulFn mul;
+    SetupFn setup;
+    int threads;   // block size
+    int smem;      // dynamic shared memory per block
+};
+
+// Threads per block for transform length 2^m: one radix-8 group per thread up to 256 threads.
+constexpr int threads_for(int m) { return m - 3 <= 5 ? 32 : (m - 3 >= 8 ? 256 : (1 << (m - 3))); }
+
+// Defined in mm_inst.cu for each m in [kMinLogN, kMaxSharedLogN].
+#define MM_DECLARE_KERNELS(M) KernelSet kernels_m##M();
+MM_DECLARE_KERNELS(2) MM_DECLARE_KERNELS(3) MM_DECLARE_KERNELS(4) MM_DECLARE_KERNELS(5)
+MM_DECLARE_KERNELS(6) MM_DECLARE_KERNELS(7) MM_DECLARE_KERNELS(8) MM_DECLARE_KERNELS(9)
+MM_DECLARE_KERNELS(10) MM_DECLARE_KERNELS(11) MM_DECLARE_KERNELS(12) MM_DECLARE_KERNELS(13)
+#undef MM_DECLARE_KERNELS
+
+}  // namespace mm

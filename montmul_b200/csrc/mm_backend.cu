@@ -1,0 +1,492 @@
+// C-ABI implementation of the B200 backend (include/montmul_b200.h): device and batch state,
+// host-side caches of x and exponents (as gpu/mod.rs:161-176, 238-270 of the reference), the
+// launch of the fused step kernels, and error reporting by status code.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/montmul_b200.h"
+#include "mm_host.hpp"
+#include "mm_abi.h"
+
+using namespace mm;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+    g_err = msg;
+    return code;
+}
+
+#define MM_CK(call)                                                                            \
+    do {                                                                                       \
+        cudaError_t e_ = (call);                                                               \
+        if (e_ != cudaSuccess) return fail(MM_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+bool kernel_set(int m, KernelSet& ks) {
+    switch (m) {
+        case 2: ks = kernels_m2(); return true;
+        case 3: ks = kernels_m3(); return true;
+        case 4: ks = kernels_m4(); return true;
+        case 5: ks = kernels_m5(); return true;
+        case 6: ks = kernels_m6(); return true;
+        case 7: ks = kernels_m7(); return true;
+        case 8: ks = kernels_m8(); return true;
+        case 9: ks = kernels_m9(); return true;
+        case 10: ks = kernels_m10(); return true;
+        case 11: ks = kernels_m11(); return true;
+        case 12: ks = kernels_m12(); return true;
+        case 13: ks = kernels_m13(); return true;
+        default: return false;
+    }
+}
+
+struct DevTables {
+    F2* t2 = nullptr;
+    F1* t1 = nullptr;
+    F2 inv8h2;
+    F1 inv8h1;
+};
+
+int log2_exact(size_t v) {
+    int l = 0;
+    while (((size_t)1 << l) < v) ++l;
+    return ((size_t)1 << l) == v ? l : -1;
+}
+
+}  // namespace
+
+struct mm_b200_device {
+    int device = 0;
+    int sms = 0;
+    int max_smem = 0;
+    int max_launch_steps = 512;
+    std::string name;
+    std::mutex mu;
+    std::map<int, DevTables> tables;
+    std::map<int, bool> configured;
+};
+
+struct mm_b200_batch {
+    mm_b200_device* dev = nullptr;
+    int m = 0;
+    size_t k = 0, n = 0, slots = 0;
+    uint32_t base = 3;
+    KernelSet ks{};
+    cudaStream_t stream = nullptr;
+    uint32_t* d_x = nullptr;
+    uint32_t* d_t = nullptr;
+    F2* d_c2 = nullptr;
+    F1* d_c1 = nullptr;
+    uint32_t* d_exp = nullptr;
+    uint32_t* d_nbits = nullptr;
+    uint32_t* d_pos = nullptr;
+    uint32_t* d_err = nullptr;
+    F2* d_spec2 = nullptr;
+    F1* d_spec1 = nullptr;
+    size_t ew = 0, exp_cap = 0;
+    const DevTables* tab = nullptr;
+    std::vector<uint32_t> host_x;
+    bool host_x_valid = true;
+    bool device_x_stale = false;
+    std::vector<std::vector<uint32_t>> exps;
+    std::vector<uint32_t> nbits, pos;
+    bool exp_dirty = false;
+    uint64_t launches = 0;
+};
+
+namespace {
+
+int ensure_tables(mm_b200_device* dev, int m, const DevTables** out) {
+    std::lock_guard<std::mutex> lock(dev->mu);
+    auto it = dev->tables.find(m);
+    if (it == dev->tables.end()) {
+        std::vector<F2> t2 = host::gen_length_tables<F2>(m);
+        std::vector<F1> t1 = host::gen_length_tables<F1>(m);
+        DevTables d;
+        MM_CK(cudaMalloc(&d.t2, t2.size() * sizeof(F2)));
+        MM_CK(cudaMalloc(&d.t1, t1.size() * sizeof(F1)));
+        MM_CK(cudaMemcpy(d.t2, t2.data(), t2.size() * sizeof(F2), cudaMemcpyHostToDevice));
+        MM_CK(cudaMemcpy(d.t1, t1.data(), t1.size() * sizeof(F1), cudaMemcpyHostToDevice));
+        d.inv8h2 = host::inv8h<F2>(m);
+        d.inv8h1 = host::inv8h<F1>(m);
+        it = dev->tables.emplace(m, d).first;
+    }
+    if (!dev->configured[m]) {
+        KernelSet ks;
+        kernel_set(m, ks);
+        MM_CK(cudaFuncSetAttribute((const void*)ks.step, cudaFuncAttributeMaxDynamicSharedMemorySize, ks.smem));
+        MM_CK(cudaFuncSetAttribute((const void*)ks.mul, cudaFuncAttributeMaxDynamicSharedMemorySize, ks.smem));
+        MM_CK(cudaFuncSetAttribute((const void*)ks.setup, cudaFuncAttributeMaxDynamicSharedMemorySize, ks.smem));
+        MM_CK(cudaFuncSetAttribute((const void*)ks.step, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                   cudaSharedmemCarveoutMaxShared));
+        dev->configured[m] = true;
+    }
+    *out = &it->second;
+    return MM_OK;
+}
+
+SlotArgs slot_args(const mm_b200_batch* b) {
+    SlotArgs a;
+    a.x = b->d_x;
+    a.tbuf = b->d_t;
+    a.c2 = b->d_c2;
+    a.c1 = b->d_c1;
+    a.exp = b->d_exp;
+    a.nbits = b->d_nbits;
+    a.pos = b->d_pos;
+    a.err = b->d_err;
+    a.tab2 = b->tab->t2;
+    a.tab1 = b->tab->t1;
+    a.ew = (uint32_t)b->ew;
+    a.base = b->base;
+    return a;
+}
+
+int pull_x(mm_b200_batch* b) {
+    if (b->host_x_valid) return MM_OK;
+    MM_CK(cudaMemcpyAsync(b->host_x.data(), b->d_x, b->host_x.size() * 4, cudaMemcpyDeviceToHost, b->stream));
+    MM_CK(cudaStreamSynchronize(b->stream));
+    b->host_x_valid = true;
+    return MM_OK;
+}
+
+// Uploads host-side changes (loaded values, exponents) before a launch (gpu/mod.rs:161-176).
+int push(mm_b200_batch* b) {
+    if (b->device_x_stale) {
+        MM_CK(cudaMemcpyAsync(b->d_x, b->host_x.data(), b->host_x.size() * 4, cudaMemcpyHostToDevice, b->stream));
+        b->device_x_stale = false;
+    }
+    if (b->exp_dirty) {
+        size_t ew = 1;
+        for (auto& e : b->exps) ew = std::max(ew, e.size());
+        std::vector<uint32_t> words(b->slots * ew, 0);
+        for (size_t i = 0; i < b->slots; ++i)
+            std::copy(b->exps[i].begin(), b->exps[i].end(), words.begin() + i * ew);
+        if (ew > b->exp_cap) {
+            if (b->d_exp) MM_CK(cudaFree(b->d_exp));
+            MM_CK(cudaMalloc(&b->d_exp, b->slots * ew * 4));
+            b->exp_cap = ew;
+        }
+        b->ew = ew;
+        MM_CK(cudaMemcpyAsync(b->d_exp, words.data(), words.size() * 4, cudaMemcpyHostToDevice, b->stream));
+        MM_CK(cudaMemcpyAsync(b->d_nbits, b->nbits.data(), b->slots * 4, cudaMemcpyHostToDevice, b->stream));
+        MM_CK(cudaMemcpyAsync(b->d_pos, b->pos.data(), b->slots * 4, cudaMemcpyHostToDevice, b->stream));
+        MM_CK(cudaStreamSynchronize(b->stream));
+        b->exp_dirty = false;
+    }
+    return MM_OK;
+}
+
+// Names the first slot whose error word is set, after clearing the words (gpu/mod.rs:178-184).
+int check_err(mm_b200_batch* b, const char* what) {
+    std::vector<uint32_t> err(b->slots);
+    MM_CK(cudaMemcpyAsync(err.data(), b->d_err, b->slots * 4, cudaMemcpyDeviceToHost, b->stream));
+    MM_CK(cudaStreamSynchronize(b->stream));
+    for (size_t i = 0; i < b->slots; ++i) {
+        if (err[i]) {
+            MM_CK(cudaMemsetAsync(b->d_err, 0, b->slots * 4, b->stream));
+            MM_CK(cudaStreamSynchronize(b->stream));
+            return fail(MM_ERR_CARRY, std::string(what) + ": carry out of a product that must fit, slot " + std::to_string(i));
+        }
+    }
+    return MM_OK;
+}
+
+int launch_steps(mm_b200_batch* b, size_t bits) {
+    size_t most = 0;
+    for (size_t i = 0; i < b->slots; ++i) most = std::max(most, (size_t)(b->nbits[i] - b->pos[i]));
+    size_t left = std::min(bits, most);
+    if (left == 0) return MM_OK;
+    int rc = push(b);
+    if (rc) return rc;
+    const SlotArgs a = slot_args(b);
+    const size_t chunk = (size_t)std::max(1, b->dev->max_launch_steps);
+    while (left > 0) {
+        const uint32_t s = (uint32_t)std::min(left, chunk);
+        b->ks.step<<<(unsigned)b->slots, b->ks.threads, b->ks.smem, b->stream>>>(a, 0, s);
+        MM_CK(cudaGetLastError());
+        ++b->launches;
+        for (size_t i = 0; i < b->slots; ++i) b->pos[i] += std::min<uint32_t>(s, b->nbits[i] - b->pos[i]);
+        left -= s;
+    }
+    b->host_x_valid = false;
+    return MM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* mm_b200_last_error(void) { return g_err.c_str(); }
+
+int mm_b200_open(const mm_b200_options* opts, mm_b200_device** out) {
+    if (!out) return fail(MM_ERR_ARG, "null output pointer");
+    mm_b200_options o{0, 0, 1, 0};
+    if (opts) o = *opts;
+    if (!o.wraparound) return fail(MM_ERR_UNSUPPORTED, "this backend runs the wraparound path only (k = L/2)");
+    if (o.force_global) return fail(MM_ERR_UNSUPPORTED, "global mode is not built in this version");
+    if (!host::check_fixed_roots()) return fail(MM_ERR_UNSUPPORTED, "field roots differ from the ones the kernels assume");
+    int count = 0;
+    MM_CK(cudaGetDeviceCount(&count));
+    if (o.device < 0 || o.device >= count) return fail(MM_ERR_ARG, "no CUDA device " + std::to_string(o.device));
+    MM_CK(cudaSetDevice(o.device));
+    cudaDeviceProp prop;
+    MM_CK(cudaGetDeviceProperties(&prop, o.device));
+    auto* d = new mm_b200_device();
+    d->device = o.device;
+    d->sms = prop.multiProcessorCount;
+    d->max_smem = (int)prop.sharedMemPerBlockOptin;
+    d->name = prop.name;
+    if (o.max_launch_steps > 0) d->max_launch_steps = o.max_launch_steps;
+    *out = d;
+    return MM_OK;
+}
+
+void mm_b200_close(mm_b200_device* dev) {
+    if (!dev) return;
+    cudaSetDevice(dev->device);
+    for (auto& kv : dev->tables) {
+        cudaFree(kv.second.t2);
+        cudaFree(kv.second.t1);
+    }
+    delete dev;
+}
+
+int mm_b200_sm_count(const mm_b200_device* dev) { return dev ? dev->sms : 0; }
+int mm_b200_max_dyn_smem(const mm_b200_device* dev) { return dev ? dev->max_smem : 0; }
+const char* mm_b200_device_name(const mm_b200_device* dev) { return dev ? dev->name.c_str() : ""; }
+
+size_t mm_b200_free_memory(mm_b200_device* dev) {
+    if (!dev) return 0;
+    cudaSetDevice(dev->device);
+    size_t free_b = 0, total = 0;
+    if (cudaMemGetInfo(&free_b, &total) != cudaSuccess) return 0;
+    return free_b;
+}
+
+void mm_b200_coefficient_bound(uint64_t out[2]) {
+    unsigned __int128 q = (unsigned __int128)P1 * P2;
+    out[0] = (uint64_t)q;
+    out[1] = (uint64_t)(q >> 64);
+}
+
+size_t mm_b200_supported_lengths(size_t* out, size_t cap) {
+    size_t cnt = 0;
+    for (int m = kMinLogN; m <= kMaxSharedLogN; ++m) {
+        if (out && cnt < cap) out[cnt] = (size_t)2 << m;
+        ++cnt;
+    }
+    return cnt;
+}
+
+int mm_b200_full_k(const mm_b200_device*) { return 1; }
+
+size_t mm_b200_batch_bytes(size_t slots, size_t len, size_t exp_words) {
+    const size_t n = len / 2;
+    // x (4n), T (8n), constants F(N') and A|B (2n elements of 24 B), exponent words, nbits,
+    // pos and err, per slot; plus mul's spectrum scratch (24n) and this length's tables.
+    const size_t per_slot = 4 * n + 8 * n + 48 * n + 4 * exp_words + 12;
+    const int m = log2_exact(n);
+    const size_t tabs = m >= kMinLogN ? (size_t)lt_size(m) * 24 : 0;
+    return slots * per_slot + 24 * n + tabs;
+}
+
+int mm_b200_create(mm_b200_device* dev, size_t k, size_t len, uint32_t base, size_t slots, const uint32_t* n,
+                   const uint32_t* nprime, const uint32_t* two_n, mm_b200_batch** out) {
+    (void)two_n;
+    if (!dev || !out || !n || !nprime) return fail(MM_ERR_ARG, "null argument");
+    if (slots == 0) return fail(MM_ERR_ARG, "empty batch");
+    const int m = log2_exact(len / 2);
+    if (len < 8 || m < kMinLogN || ((size_t)2 << m) != len) return fail(MM_ERR_ARG, "transform length must be a power of two >= 8");
+    if (m > kMaxSharedLogN) return fail(MM_ERR_UNSUPPORTED, "transform length " + std::to_string(len) + " needs global mode, not built in this version");
+    if (k != len / 2) return fail(MM_ERR_ARG, "wraparound needs k = L/2");
+    if (base < 1 || base > 4) return fail(MM_ERR_ARG, "base must be in 1..4 (lazy range)");
+    MM_CK(cudaSetDevice(dev->device));
+    const size_t need = mm_b200_batch_bytes(slots, len, 1) + 8 * slots * k + ((size_t)64 << 20);
+    const size_t freeb = mm_b200_free_memory(dev);
+    if (need > freeb) return fail(MM_ERR_OOM, "batch needs " + std::to_string(need) + " bytes, " + std::to_string(freeb) + " free");
+    const DevTables* tab = nullptr;
+    int rc = ensure_tables(dev, m, &tab);
+    if (rc) return rc;
+    std::unique_ptr<mm_b200_batch> b(new mm_b200_batch());
+    b->dev = dev;
+    b->m = m;
+    b->k = k;
+    b->n = len / 2;
+    b->slots = slots;
+    b->base = base;
+    b->tab = tab;
+    kernel_set(m, b->ks);
+    MM_CK(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+    const size_t nn = b->n;
+    MM_CK(cudaMalloc(&b->d_x, slots * k * 4));
+    MM_CK(cudaMalloc(&b->d_t, slots * 2 * nn * 4));
+    MM_CK(cudaMalloc(&b->d_c2, slots * 2 * nn * sizeof(F2)));
+    MM_CK(cudaMalloc(&b->d_c1, slots * 2 * nn * sizeof(F1)));
+    MM_CK(cudaMalloc(&b->d_exp, slots * 4));
+    b->exp_cap = 1;
+    b->ew = 1;
+    MM_CK(cudaMalloc(&b->d_nbits, slots * 4));
+    MM_CK(cudaMalloc(&b->d_pos, slots * 4));
+    MM_CK(cudaMalloc(&b->d_err, slots * 4));
+    MM_CK(cudaMalloc(&b->d_spec2, nn * sizeof(F2)));
+    MM_CK(cudaMalloc(&b->d_spec1, nn * sizeof(F1)));
+    MM_CK(cudaMemsetAsync(b->d_x, 0, slots * k * 4, b->stream));
+    MM_CK(cudaMemsetAsync(b->d_exp, 0, slots * 4, b->stream));
+    MM_CK(cudaMemsetAsync(b->d_nbits, 0, slots * 4, b->stream));
+    MM_CK(cudaMemsetAsync(b->d_pos, 0, slots * 4, b->stream));
+    MM_CK(cudaMemsetAsync(b->d_err, 0, slots * 4, b->stream));
+    // Per-slot constants from N and N' on the device.
+    uint32_t *d_n = nullptr, *d_np = nullptr;
+    MM_CK(cudaMalloc(&d_n, slots * k * 4));
+    MM_CK(cudaMalloc(&d_np, slots * k * 4));
+    MM_CK(cudaMemcpyAsync(d_n, n, slots * k * 4, cudaMemcpyHostToDevice, b->stream));
+    MM_CK(cudaMemcpyAsync(d_np, nprime, slots * k * 4, cudaMemcpyHostToDevice, b->stream));
+    for (size_t first = 0; first < slots; first += 65535) {
+        const unsigned grid = (unsigned)std::min<size_t>(65535, slots - first);
+        b->ks.setup<<<grid, b->ks.threads, b->ks.smem, b->stream>>>(d_n, d_np, b->d_c2, b->d_c1, tab->t2, tab->t1, tab->inv8h2,
+                                                                   tab->inv8h1, (uint32_t)first);
+        MM_CK(cudaGetLastError());
+        ++b->launches;
+    }
+    MM_CK(cudaStreamSynchronize(b->stream));
+    MM_CK(cudaFree(d_n));
+    MM_CK(cudaFree(d_np));
+    b->host_x.assign(slots * k, 0);
+    b->host_x_valid = true;
+    b->device_x_stale = false;
+    b->exps.assign(slots, std::vector<uint32_t>());
+    b->nbits.assign(slots, 0);
+    b->pos.assign(slots, 0);
+    *out = b.release();
+    return MM_OK;
+}
+
+int mm_b200_load(mm_b200_batch* b, size_t i, const uint32_t* limbs) {
+    if (!b || !limbs || i >= b->slots) return fail(MM_ERR_ARG, "load: bad slot");
+    int rc = pull_x(b);
+    if (rc) return rc;
+    std::memcpy(b->host_x.data() + i * b->k, limbs, b->k * 4);
+    b->device_x_stale = true;
+    return MM_OK;
+}
+
+int mm_b200_load_all(mm_b200_batch* b, const uint32_t* limbs) {
+    if (!b || !limbs) return fail(MM_ERR_ARG, "load_all: null argument");
+    std::memcpy(b->host_x.data(), limbs, b->host_x.size() * 4);
+    b->host_x_valid = true;
+    b->device_x_stale = true;
+    return MM_OK;
+}
+
+int mm_b200_set_exponent(mm_b200_batch* b, size_t i, const uint32_t* words, size_t nwords, size_t nbits) {
+    if (!b || i >= b->slots) return fail(MM_ERR_ARG, "set_exponent: bad slot");
+    if (nbits > 32 * nwords || nbits > 0xffffffffu || (nwords && !words)) return fail(MM_ERR_ARG, "set_exponent: nbits exceeds the words");
+    b->exps[i].assign(words, words + nwords);
+    b->nbits[i] = (uint32_t)nbits;
+    b->pos[i] = 0;
+    b->exp_dirty = true;
+    return MM_OK;
+}
+
+int mm_b200_set_exponents(mm_b200_batch* b, const uint32_t* words, size_t ew, const uint32_t* nbits) {
+    if (!b || (!words && ew) || !nbits) return fail(MM_ERR_ARG, "set_exponents: null argument");
+    for (size_t i = 0; i < b->slots; ++i) {
+        if (nbits[i] > 32 * ew) return fail(MM_ERR_ARG, "set_exponents: nbits exceeds the words");
+        b->exps[i].assign(words + i * ew, words + (i + 1) * ew);
+        b->nbits[i] = nbits[i];
+        b->pos[i] = 0;
+    }
+    b->exp_dirty = true;
+    return MM_OK;
+}
+
+int mm_b200_run_async(mm_b200_batch* b, size_t bits) {
+    if (!b) return fail(MM_ERR_ARG, "run: null batch");
+    MM_CK(cudaSetDevice(b->dev->device));
+    return launch_steps(b, bits);
+}
+
+int mm_b200_sync(mm_b200_batch* b) {
+    if (!b) return fail(MM_ERR_ARG, "sync: null batch");
+    MM_CK(cudaStreamSynchronize(b->stream));
+    return check_err(b, "run");
+}
+
+int mm_b200_run(mm_b200_batch* b, size_t bits) {
+    int rc = mm_b200_run_async(b, bits);
+    if (rc) return rc;
+    return mm_b200_sync(b);
+}
+
+int mm_b200_mul(mm_b200_batch* b, size_t out, size_t a, size_t bb) {
+    if (!b || out >= b->slots || a >= b->slots || bb >= b->slots) return fail(MM_ERR_ARG, "mul: bad slot");
+    MM_CK(cudaSetDevice(b->dev->device));
+    int rc = push(b);
+    if (rc) return rc;
+    b->ks.mul<<<1, b->ks.threads, b->ks.smem, b->stream>>>(slot_args(b), (uint32_t)out, (uint32_t)a, (uint32_t)bb, b->d_spec2,
+                                                          b->d_spec1);
+    MM_CK(cudaGetLastError());
+    ++b->launches;
+    MM_CK(cudaStreamSynchronize(b->stream));
+    b->host_x_valid = false;
+    return check_err(b, "mul");
+}
+
+int mm_b200_read(mm_b200_batch* b, size_t i, uint32_t* limbs) {
+    if (!b || !limbs || i >= b->slots) return fail(MM_ERR_ARG, "read: bad slot");
+    int rc = pull_x(b);
+    if (rc) return rc;
+    std::memcpy(limbs, b->host_x.data() + i * b->k, b->k * 4);
+    return MM_OK;
+}
+
+int mm_b200_read_all(mm_b200_batch* b, uint32_t* limbs) {
+    if (!b || !limbs) return fail(MM_ERR_ARG, "read_all: null argument");
+    int rc = pull_x(b);
+    if (rc) return rc;
+    std::memcpy(limbs, b->host_x.data(), b->host_x.size() * 4);
+    return MM_OK;
+}
+
+size_t mm_b200_remaining(const mm_b200_batch* b, size_t i) {
+    if (!b || i >= b->slots) return 0;
+    return b->nbits[i] - b->pos[i];
+}
+
+size_t mm_b200_slots(const mm_b200_batch* b) { return b ? b->slots : 0; }
+
+void* mm_b200_stream(mm_b200_batch* b) { return b ? (void*)b->stream : nullptr; }
+
+uint64_t mm_b200_launches(const mm_b200_batch* b) { return b ? b->launches : 0; }
+
+void mm_b200_destroy(mm_b200_batch* b) {
+    if (!b) return;
+    cudaSetDevice(b->dev->device);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    cudaFree(b->d_x);
+    cudaFree(b->d_t);
+    cudaFree(b->d_c2);
+    cudaFree(b->d_c1);
+    cudaFree(b->d_exp);
+    cudaFree(b->d_nbits);
+    cudaFree(b->d_pos);
+    cudaFree(b->d_err);
+    cudaFree(b->d_spec2);
+    cudaFree(b->d_spec1);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+}
+
+}  // extern "C"

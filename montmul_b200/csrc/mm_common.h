@@ -1,0 +1,98 @@
+// Shared host/device definitions of the B200 MontMul backend: field constants, element types,
+// the per-length transform schedule (radix of every pass) and the layout of the twiddle tables.
+//
+// The transform is the reference's right-angle NTT over GF(M31^2) x GF(M61^2)
+// (montmul/src/field.rs, cpu.rs:49-115): a length-n complex DIF (natural order in, bit-reversed
+// order out) and DIT (bit-reversed in, natural out), n = L/2. Here it runs as radix-8/4/2
+// passes; a radix-R pass is exactly R' = log2 R consecutive radix-2 stages of the reference,
+// so every spectrum position holds the same value as in the reference.
+#pragma once
+#include <stdint.h>
+
+#if defined(__CUDACC__)
+#define MM_HD __host__ __device__ __forceinline__
+#else
+#define MM_HD inline
+#endif
+
+namespace mm {
+
+constexpr uint32_t P1 = 0x7fffffffu;             // M31
+constexpr uint64_t P2 = 0x1fffffffffffffffull;   // M61
+
+struct __align__(8) F1 { uint32_t re, im; };
+struct __align__(16) F2 { uint64_t re, im; };
+
+// Largest transform length handled with the whole vector in shared memory: n = 8192
+// (L = 16384) needs 24 n = 196,608 B of the 227 KB a B200 block may opt into.
+constexpr int kMaxSharedLogN = 13;
+constexpr int kMinLogN = 2;   // L = 8
+
+// ---- pass schedule: radices, DIF order ----
+// m = log2 n. m = 3a -> [8]*a; m = 3a + 1 -> [4, 4, 8*(a-1)]; m = 3a + 2 -> [4, 8*a];
+// m = 1 -> [2], m = 2 -> [4]. Radix-8 passes dominate; the last DIF pass (span 1) carries no
+// twiddles, so it is kept at radix 8 whenever m >= 3.
+MM_HD constexpr int sched_passes(int m) {
+    return m <= 3 ? 1 : (m % 3 == 0 ? m / 3 : (m % 3 == 1 ? m / 3 + 1 : m / 3 + 1));
+}
+MM_HD constexpr int sched_radix(int m, int i) {
+    return m == 1 ? 2 : m == 2 ? 4 : m == 3 ? 8
+         : (m % 3 == 0 ? 8 : (m % 3 == 1 ? (i < 2 ? 4 : 8) : (i < 1 ? 4 : 8)));
+}
+MM_HD constexpr int ilog2c(int v) { return v <= 1 ? 0 : 1 + ilog2c(v / 2); }
+// Span q of the last radix-2 stage of DIF pass i (also the first span of the DIT pass i).
+MM_HD constexpr int sched_q(int m, int i) {
+    int lq = m;
+    for (int p = 0; p <= i; ++p) lq -= ilog2c(sched_radix(m, p));
+    return 1 << lq;
+}
+
+// ---- twiddle table layout for one transform (m, weighted) ----
+// Elements (F1 and F2 arrays use the same indices):
+//   forward pass i with q_i > 1:  weighted pass 0: R*q entries [k][j] = zeta^j W^(j rev_R(k));
+//                                 other passes:    (R-1)*q entries [k-1][j] = W^(j rev_R(k)).
+//   inverse pass i with q_i > 1:  same shapes with V = W^-1 (and zeta^-j for weighted pass 0).
+//   weighted transforms then hold R_0 input constants zeta^(q_0 k) and R_0 output constants
+//   zeta^(-q_0 k) / n.
+// W is the primitive (R q)-th root omega_n^(n/(R q)) of the reference's tables (field.rs:243).
+MM_HD constexpr int tab_pass_size(int m, int i, bool weighted) {
+    int R = sched_radix(m, i), q = sched_q(m, i);
+    return q <= 1 ? 0 : (weighted && i == 0 ? R * q : (R - 1) * q);
+}
+MM_HD constexpr int tab_fwd_off(int m, int i, bool weighted) {
+    int o = 0;
+    for (int p = 0; p < i; ++p) o += tab_pass_size(m, p, weighted);
+    return o;
+}
+MM_HD constexpr int tab_fwd_size(int m, bool weighted) { return tab_fwd_off(m, sched_passes(m), weighted); }
+MM_HD constexpr int tab_inv_off(int m, int i, bool weighted) {
+    return tab_fwd_size(m, weighted) + tab_fwd_off(m, i, weighted);
+}
+MM_HD constexpr int tab_in_const_off(int m, bool weighted) { return 2 * tab_fwd_size(m, weighted); }
+MM_HD constexpr int tab_out_const_off(int m, bool weighted) {
+    return tab_in_const_off(m, weighted) + (weighted ? sched_radix(m, 0) : 0);
+}
+MM_HD constexpr int tab_size(int m, bool weighted) {
+    return tab_out_const_off(m, weighted) + (weighted ? sched_radix(m, 0) : 0);
+}
+
+// Tables of one transform length L = 2^(m+1): the weighted length-n transform (m = log2 n)
+// followed by the unweighted length-h transform of the wraparound path (h = n/2), then the
+// wraparound set-up tables u[p] = w^rev(p), iu[p] = w^-rev(p) over h positions (cpu.rs:165-179).
+MM_HD constexpr int lt_full_off(int) { return 0; }
+MM_HD constexpr int lt_half_off(int m) { return tab_size(m, true); }
+MM_HD constexpr int lt_unpack_off(int m) { return lt_half_off(m) + (m >= 2 ? tab_size(m - 1, false) : 0); }
+MM_HD constexpr int lt_size(int m) { return lt_unpack_off(m) + 2 * (1 << (m - 1)); }
+
+// Per-slot constants in the order the fused pointwise step reads them: the spectrum position
+// p = R*g + k of the last DIF pass (radix R = sched_radix(m, last)) is stored at k*(n/R) + g,
+// so the R loads of one group are coalesced across a warp. n elements hold N^' = F(N'); the
+// next n hold the wraparound factors A (positions p < h) and B (h + p), in natural position
+// order (cpu.rs:265-284).
+MM_HD constexpr int const_index(int m, int p) {
+    int R = sched_radix(m, sched_passes(m) - 1);
+    int n = 1 << m;
+    return (p % R) * (n / R) + p / R;
+}
+
+}  // namespace mm

@@ -1,0 +1,144 @@
+// Device arithmetic in GF(M31), GF(M61) and their quadratic extensions with i^2 = -1
+// (montmul/src/field.rs:13-42, 131-222). All results are canonical (in [0, p)), so every value
+// equals the reference's bit for bit.
+//
+// Two facts of the reference's tables make the radix-8 butterflies cheap: in both fields the
+// primitive 4th root used by the transforms is omega^(n/4) = i, and the primitive 8th root is
+// omega^(n/8) = (1 + i) * 2^s with s = 15 (M31) or 30 (M61), so a product with an 8th root is
+// one add, one sub and a bit rotation (2^s * x mod 2^b - 1 rotates x by s bits). The host
+// checks both facts against its own tables before any launch.
+#pragma once
+#include "mm_common.h"
+
+namespace mm {
+
+// ---- GF(M31) ----
+__device__ __forceinline__ uint32_t add1(uint32_t a, uint32_t b) {
+    uint32_t s = a + b;
+    return min(s, s - P1);
+}
+__device__ __forceinline__ uint32_t sub1(uint32_t a, uint32_t b) {
+    uint32_t d = a - b;
+    return min(d, d + P1);
+}
+// t mod M31 for t < 2^63.
+__device__ __forceinline__ uint32_t red1(uint64_t t) {
+    uint64_t u = (t & P1) + (t >> 31);                  // < 2^33
+    uint32_t v = (uint32_t)(u & P1) + (uint32_t)(u >> 31);  // < 2^31 + 4
+    return min(v, v - P1);
+}
+__device__ __forceinline__ uint32_t mul1(uint32_t a, uint32_t b) {
+    uint64_t t = (uint64_t)a * b;                       // < 2^62
+    uint32_t s = (uint32_t)(t & P1) + (uint32_t)(t >> 31);
+    return min(s, s - P1);
+}
+// x * 2^15 mod M31 (rotation of the 31-bit string).
+__device__ __forceinline__ uint32_t rot1(uint32_t x) { return ((x << 15) & P1) | (x >> 16); }
+// x * 2 mod M31.
+__device__ __forceinline__ uint32_t dbl1(uint32_t x) { return ((x << 1) & P1) | (x >> 30); }
+
+// ---- GF(M61) ----
+__device__ __forceinline__ uint64_t add2(uint64_t a, uint64_t b) {
+    uint64_t s = a + b;
+    return min(s, s - P2);
+}
+__device__ __forceinline__ uint64_t sub2(uint64_t a, uint64_t b) {
+    uint64_t d = a - b;
+    return min(d, d + P2);
+}
+// (hi:lo) mod M61 for hi:lo < 2^124.
+__device__ __forceinline__ uint64_t red2(uint64_t lo, uint64_t hi) {
+    uint64_t t = (lo & P2) + ((hi << 3) | (lo >> 61));  // < 2^61 + 2^63
+    uint64_t s = (t & P2) + (t >> 61);                   // < 2^61 + 4
+    return min(s, s - P2);
+}
+__device__ __forceinline__ uint64_t mul2(uint64_t a, uint64_t b) {
+    uint64_t lo = a * b, hi = __umul64hi(a, b);
+    uint64_t s = (lo & P2) + ((hi << 3) | (lo >> 61));   // <= 2 P2
+    return min(s, s - P2);
+}
+// a*b + c*d mod M61 for canonical inputs (the sum is below 2^123).
+__device__ __forceinline__ uint64_t mul2x2(uint64_t a, uint64_t b, uint64_t c, uint64_t d) {
+    uint64_t lo1 = a * b, hi1 = __umul64hi(a, b);
+    uint64_t lo2 = c * d, hi2 = __umul64hi(c, d);
+    uint64_t lo = lo1 + lo2;
+    uint64_t hi = hi1 + hi2 + (lo < lo1);
+    return red2(lo, hi);
+}
+__device__ __forceinline__ uint64_t rot2(uint64_t x) { return ((x << 30) & P2) | (x >> 31); }
+
+// ---- GF(M31^2) ----
+__device__ __forceinline__ F1 f1(uint32_t re, uint32_t im) { F1 r; r.re = re; r.im = im; return r; }
+__device__ __forceinline__ F1 cadd(F1 a, F1 b) { return f1(add1(a.re, b.re), add1(a.im, b.im)); }
+__device__ __forceinline__ F1 csub(F1 a, F1 b) { return f1(sub1(a.re, b.re), sub1(a.im, b.im)); }
+// (a - b) * i
+__device__ __forceinline__ F1 csub_i(F1 a, F1 b) { return f1(sub1(b.im, a.im), sub1(a.re, b.re)); }
+// (a - b) * (-i)
+__device__ __forceinline__ F1 csub_mi(F1 a, F1 b) { return f1(sub1(a.im, b.im), sub1(b.re, a.re)); }
+__device__ __forceinline__ F1 cmul(F1 a, F1 b) {
+    uint64_t re = (uint64_t)a.re * b.re + (uint64_t)a.im * (P1 - b.im);
+    uint64_t im = (uint64_t)a.re * b.im + (uint64_t)a.im * b.re;
+    return f1(red1(re), red1(im));
+}
+// real * complex
+__device__ __forceinline__ F1 cmul_r(uint32_t a, F1 b) { return f1(mul1(a, b.re), mul1(a, b.im)); }
+// re(a * b)
+__device__ __forceinline__ uint32_t cmul_re(F1 a, F1 b) {
+    return red1((uint64_t)a.re * b.re + (uint64_t)a.im * (P1 - b.im));
+}
+__device__ __forceinline__ F1 csqr(F1 a) {
+    uint32_t m = mul1(a.re, a.im);
+    return f1(mul1(add1(a.re, a.im), sub1(a.re, a.im)), add1(m, m));
+}
+__device__ __forceinline__ F1 cscale(F1 a, uint32_t c) {  // c <= 4
+    return f1(red1((uint64_t)a.re * c), red1((uint64_t)a.im * c));
+}
+__device__ __forceinline__ F1 cconj(F1 a) { return f1(a.re, sub1(0, a.im)); }
+// x * omega_8 = x * (1 + i) 2^15
+__device__ __forceinline__ F1 mul_w8(F1 x) { return f1(rot1(sub1(x.re, x.im)), rot1(add1(x.re, x.im))); }
+// x * omega_8^-1 = x * (1 - i) 2^15
+__device__ __forceinline__ F1 mul_v8(F1 x) { return f1(rot1(add1(x.re, x.im)), rot1(sub1(x.im, x.re))); }
+__device__ __forceinline__ F1 mul_i(F1 x) { return f1(sub1(0, x.im), x.re); }
+__device__ __forceinline__ F1 mul_mi(F1 x) { return f1(x.im, sub1(0, x.re)); }
+
+// ---- GF(M61^2) ----
+__device__ __forceinline__ F2 f2(uint64_t re, uint64_t im) { F2 r; r.re = re; r.im = im; return r; }
+__device__ __forceinline__ F2 cadd(F2 a, F2 b) { return f2(add2(a.re, b.re), add2(a.im, b.im)); }
+__device__ __forceinline__ F2 csub(F2 a, F2 b) { return f2(sub2(a.re, b.re), sub2(a.im, b.im)); }
+__device__ __forceinline__ F2 csub_i(F2 a, F2 b) { return f2(sub2(b.im, a.im), sub2(a.re, b.re)); }
+__device__ __forceinline__ F2 csub_mi(F2 a, F2 b) { return f2(sub2(a.im, b.im), sub2(b.re, a.re)); }
+__device__ __forceinline__ F2 cmul(F2 a, F2 b) {
+    return f2(mul2x2(a.re, b.re, a.im, P2 - b.im), mul2x2(a.re, b.im, a.im, b.re));
+}
+__device__ __forceinline__ F2 cmul_r(uint64_t a, F2 b) { return f2(mul2(a, b.re), mul2(a, b.im)); }
+__device__ __forceinline__ uint64_t cmul_re(F2 a, F2 b) { return mul2x2(a.re, b.re, a.im, P2 - b.im); }
+__device__ __forceinline__ F2 csqr(F2 a) {
+    uint64_t m = mul2(a.re, a.im);
+    return f2(mul2(add2(a.re, a.im), sub2(a.re, a.im)), add2(m, m));
+}
+__device__ __forceinline__ uint64_t scale2(uint64_t a, uint32_t c) {   // c <= 4, a < 2^61
+    uint64_t t = a * c;                                   // < 2^63
+    uint64_t s = (t & P2) + (t >> 61);
+    return min(s, s - P2);
+}
+__device__ __forceinline__ F2 cscale(F2 a, uint32_t c) { return f2(scale2(a.re, c), scale2(a.im, c)); }
+__device__ __forceinline__ F2 cconj(F2 a) { return f2(a.re, sub2(0, a.im)); }
+__device__ __forceinline__ F2 mul_w8(F2 x) { return f2(rot2(sub2(x.re, x.im)), rot2(add2(x.re, x.im))); }
+__device__ __forceinline__ F2 mul_v8(F2 x) { return f2(rot2(add2(x.re, x.im)), rot2(sub2(x.im, x.re))); }
+__device__ __forceinline__ F2 mul_i(F2 x) { return f2(sub2(0, x.im), x.re); }
+__device__ __forceinline__ F2 mul_mi(F2 x) { return f2(x.im, sub2(0, x.re)); }
+
+// ---- CRT (field.rs:288-294) ----
+// The unique C < M31 * M61 with C = c1 mod M31 and C = c2 mod M61, as three 32-bit words.
+// (M61 mod M31)^-1 = -2 mod M31, so h = 2 (c2 mod M31 - c1) mod M31 and C = c2 + M61 h.
+__device__ __forceinline__ void crt3(uint32_t c1, uint64_t c2, uint32_t& w0, uint32_t& w1, uint32_t& w2) {
+    uint32_t c2m = (uint32_t)(c2 & P1) + (uint32_t)(c2 >> 31);   // < 2^31 + 2^30
+    c2m = min(c2m, c2m - P1);
+    uint32_t h = dbl1(sub1(c2m, c1));
+    unsigned __int128 v = (unsigned __int128)c2 + ((unsigned __int128)h << 61) - h;
+    w0 = (uint32_t)v;
+    w1 = (uint32_t)(v >> 32);
+    w2 = (uint32_t)(v >> 64);
+}
+
+}  // namespace mm

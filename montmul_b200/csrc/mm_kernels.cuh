@@ -1,0 +1,247 @@
+// The fused modular step and its set-up, one thread block per slot with the whole vector in
+// shared memory (n <= 8192 elements of 24 bytes).
+//
+// One step (montmul/src/cpu.rs:486-497 with redc 452-484, wraparound path):
+//   T = c x^2:       forward(x) -> square * c -> inverse -> carry into T (2k limbs, global)
+//   m = T N' mod R:  forward(T mod R) -> * F(N') -> inverse -> carry (low k limbs), packed
+//   m N mod (R-1):   half-length DIF -> e A + d B (cpu.rs:261-284) -> half-length DIT
+//   x = T/R + ((m N + T mod R) mod (R - 1))  with the end-around carry, then + T high half.
+// The exponent bit of every step is read on the device (transform.rs:67).
+#pragma once
+#include "mm_abi.h"
+#include "mm_carry.cuh"
+
+namespace mm {
+
+// ---- pointwise operations of the fused pass (positions R g + k) ----
+// apply2/apply1 transform the R values of group g in place; returning true stops the pass
+// before the inverse butterflies (the spectrum was consumed).
+struct SquareOp {
+    uint32_t c;
+    template <int R> __device__ __forceinline__ bool apply2(F2* x, int) const {
+#pragma unroll
+        for (int k = 0; k < R; ++k) { x[k] = csqr(x[k]); if (c != 1) x[k] = cscale(x[k], c); }
+        return false;
+    }
+    template <int R> __device__ __forceinline__ bool apply1(F1* x, int) const {
+#pragma unroll
+        for (int k = 0; k < R; ++k) { x[k] = csqr(x[k]); if (c != 1) x[k] = cscale(x[k], c); }
+        return false;
+    }
+};
+
+// Multiplies by a spectrum stored in fused-pass order (element k * (n / R) + g).
+template <int M> struct SpecMulOp {
+    const F2* b2; const F1* b1;
+    template <int R> __device__ __forceinline__ bool apply2(F2* x, int g) const {
+#pragma unroll
+        for (int k = 0; k < R; ++k) x[k] = cmul(x[k], b2[k * ((1 << M) / R) + g]);
+        return false;
+    }
+    template <int R> __device__ __forceinline__ bool apply1(F1* x, int g) const {
+#pragma unroll
+        for (int k = 0; k < R; ++k) x[k] = cmul(x[k], b1[k * ((1 << M) / R) + g]);
+        return false;
+    }
+};
+
+// Stores the spectrum in fused-pass order and stops (no inverse).
+template <int M> struct SpecStoreOp {
+    F2* b2; F1* b1;
+    template <int R> __device__ __forceinline__ bool apply2(F2* x, int g) const {
+#pragma unroll
+        for (int k = 0; k < R; ++k) b2[k * ((1 << M) / R) + g] = x[k];
+        return true;
+    }
+    template <int R> __device__ __forceinline__ bool apply1(F1* x, int g) const {
+#pragma unroll
+        for (int k = 0; k < R; ++k) b1[k * ((1 << M) / R) + g] = x[k];
+        return true;
+    }
+};
+
+// ---- the wraparound half-pointwise step (cpu.rs:221-237, 261-284) ----
+// out_p = (z_p + conj z_q) A_p + (z_p - conj z_q) B_p with q = partner(p), the position of
+// index (h - rev(p)) mod h; in place, one thread per pair {p, q} (q = 3 * 2^a - 1 - p for p in
+// octave [2^a, 2^(a+1)), q = p for p < 2).
+template <int MH, int NT>
+__device__ __forceinline__ void half_pointwise(F2* s2, F1* s1, const F2* __restrict__ ab2, const F1* __restrict__ ab1) {
+    constexpr int H = 1 << MH;
+    for (int tau = threadIdx.x; tau < H / 2 + 1; tau += NT) {
+        const int p = tau < 2 ? tau : tau - 1 + (1 << (31 - __clz(tau - 1)));
+        const int q = p == 0 ? 0 : (3 << (31 - __clz(p))) - 1 - p;
+        {
+            const F2 zp = s2[swz(p)], zq = s2[swz(q)];
+            const F2 e = cadd(zp, cconj(zq)), d = csub(zp, cconj(zq));
+            const F2 op = cadd(cmul(e, ab2[p]), cmul(d, ab2[H + p]));
+            if (q != p) {
+                const F2 e2 = cadd(zq, cconj(zp)), d2 = csub(zq, cconj(zp));
+                s2[swz(q)] = cadd(cmul(e2, ab2[q]), cmul(d2, ab2[H + q]));
+            }
+            s2[swz(p)] = op;
+        }
+        {
+            const F1 zp = s1[swz(p)], zq = s1[swz(q)];
+            const F1 e = cadd(zp, cconj(zq)), d = csub(zp, cconj(zq));
+            const F1 op = cadd(cmul(e, ab1[p]), cmul(d, ab1[H + p]));
+            if (q != p) {
+                const F1 e2 = cadd(zq, cconj(zp)), d2 = csub(zq, cconj(zp));
+                s1[swz(q)] = cadd(cmul(e2, ab1[q]), cmul(d2, ab1[H + q]));
+            }
+            s1[swz(p)] = op;
+        }
+    }
+    __syncthreads();
+}
+
+// Shared memory of one block: F2 vector (16 n B), F1 vector (8 n B).
+template <int M> constexpr int smem_bytes() { return 24 << M; }
+
+// REDC from T (in tl, 2n limbs) into x (n limbs), wraparound path. Returns false on a carry
+// out that must vanish.
+template <int M, int NT>
+__device__ __forceinline__ bool redc_wrap(F2* s2, F1* s1, const uint32_t* tl, uint32_t* x, const F2* cc2, const F1* cc1,
+                                          const F2* tab2, const F1* tab1, uint64_t* sc) {
+    constexpr int N = 1 << M;
+    const F2* ht2 = tab2 + lt_half_off(M);
+    const F1* ht1 = tab1 + lt_half_off(M);
+    fwd_limbs<M, NT>(tl, N, s2, s1, tab2, tab1);
+    fused_mid<M, NT, true>(tl, N, s2, s1, tab2, tab1, SpecMulOp<M>{cc2, cc1});
+    inv_to_natural<M, NT, true>(s2, s1, tab2, tab1);
+    carry_low_and_pack<M, NT>(s2, s1, sc);
+    dif_unweighted<M - 1, NT>(s2, s1, ht2, ht1);
+    half_pointwise<M - 1, NT>(s2, s1, cc2 + N, cc1 + N);
+    dit_unweighted<M - 1, NT>(s2, s1, ht2, ht1);
+    return wrap_combine<M, NT>(s2, s1, tl, x, sc);
+}
+
+// Up to `bits` steps x <- x^2 c^bit R^-1 on slot first + blockIdx.x (cpu.rs:543-556).
+template <int M, int NT>
+__global__ void __launch_bounds__(NT, (M <= 12 ? 2 : 1)) step_kernel(SlotArgs a, uint32_t first, uint32_t bits) {
+    constexpr int N = 1 << M;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    F2* s2 = reinterpret_cast<F2*>(smem_raw);
+    F1* s1 = reinterpret_cast<F1*>(smem_raw + 16 * N);
+    __shared__ uint64_t sc[CarryScratch<NT>::words];
+    const uint32_t slot = first + blockIdx.x;
+    uint32_t* x = a.x + (size_t)slot * N;
+    uint32_t* tl = a.tbuf + (size_t)slot * 2 * N;
+    const F2* cc2 = a.c2 + (size_t)slot * 2 * N;
+    const F1* cc1 = a.c1 + (size_t)slot * 2 * N;
+    const uint32_t* ex = a.exp + (size_t)slot * a.ew;
+    const uint32_t nb = a.nbits[slot];
+    uint32_t pos = a.pos[slot];
+    bool ok = true;
+    for (uint32_t it = 0; it < bits && pos < nb; ++it, ++pos) {
+        const uint32_t bit = (ex[pos >> 5] >> (31 - (pos & 31))) & 1;
+        const uint32_t c = bit ? a.base : 1;
+        fwd_limbs<M, NT>(x, N, s2, s1, a.tab2, a.tab1);
+        fused_mid<M, NT, false>(x, N, s2, s1, a.tab2, a.tab1, SquareOp{c});
+        inv_to_natural<M, NT, false>(s2, s1, a.tab2, a.tab1);
+        ok &= carry_product<M, NT>(s2, s1, tl, sc) == 0;
+        ok &= redc_wrap<M, NT>(s2, s1, tl, x, cc2, cc1, a.tab2, a.tab1, sc);
+    }
+    if (threadIdx.x == 0) {
+        a.pos[slot] = pos;
+        if (!ok) a.err[slot] = 1;
+    }
+}
+
+// x[out] <- x[ia] x[ib] R^-1 with slot out's modulus (cpu.rs:558-571), one block. spec: n
+// elements of scratch for F(x[ib]).
+template <int M, int NT>
+__global__ void __launch_bounds__(NT) mul_kernel(SlotArgs a, uint32_t out, uint32_t ia, uint32_t ib, F2* spec2, F1* spec1) {
+    constexpr int N = 1 << M;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    F2* s2 = reinterpret_cast<F2*>(smem_raw);
+    F1* s1 = reinterpret_cast<F1*>(smem_raw + 16 * N);
+    __shared__ uint64_t sc[CarryScratch<NT>::words];
+    const uint32_t* xb = a.x + (size_t)ib * N;
+    const uint32_t* xa = a.x + (size_t)ia * N;
+    fwd_limbs<M, NT>(xb, N, s2, s1, a.tab2, a.tab1);
+    fused_mid<M, NT, false>(xb, N, s2, s1, a.tab2, a.tab1, SpecStoreOp<M>{spec2, spec1});
+    __syncthreads();
+    fwd_limbs<M, NT>(xa, N, s2, s1, a.tab2, a.tab1);
+    fused_mid<M, NT, false>(xa, N, s2, s1, a.tab2, a.tab1, SpecMulOp<M>{spec2, spec1});
+    inv_to_natural<M, NT, false>(s2, s1, a.tab2, a.tab1);
+    uint32_t* tl = a.tbuf + (size_t)out * 2 * N;
+    bool ok = carry_product<M, NT>(s2, s1, tl, sc) == 0;
+    ok &= redc_wrap<M, NT>(s2, s1, tl, a.x + (size_t)out * N, a.c2 + (size_t)out * 2 * N, a.c1 + (size_t)out * 2 * N,
+                           a.tab2, a.tab1, sc);
+    if (threadIdx.x == 0 && !ok) a.err[out] = 1;
+}
+
+// Per-slot constants of slot first + blockIdx.x from its N and N' limbs (k = n each):
+// F(N') in fused-pass order (cpu.rs:518), then the wraparound factors A | B from the half
+// transform of N (cpu.rs:239-284; computed on the host by the reference's GPU backend).
+// inv8h = (8 h)^-1 in each field.
+template <int M, int NT>
+__global__ void __launch_bounds__(NT) setup_kernel(const uint32_t* nl, const uint32_t* npl, F2* c2, F1* c1, const F2* tab2,
+                                                   const F1* tab1, F2 inv8h2, F1 inv8h1, uint32_t first) {
+    constexpr int N = 1 << M, H = N / 2;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    F2* s2 = reinterpret_cast<F2*>(smem_raw);
+    F1* s1 = reinterpret_cast<F1*>(smem_raw + 16 * N);
+    const uint32_t slot = first + blockIdx.x;
+    const uint32_t* np = npl + (size_t)slot * N;
+    const uint32_t* nn = nl + (size_t)slot * N;
+    F2* o2 = c2 + (size_t)slot * 2 * N;
+    F1* o1 = c1 + (size_t)slot * 2 * N;
+    fwd_limbs<M, NT>(np, N, s2, s1, tab2, tab1);
+    fused_mid<M, NT, false>(np, N, s2, s1, tab2, tab1, SpecStoreOp<M>{o2, o1});
+    __syncthreads();
+    // half_forward (cpu.rs:286-295): z_j = N_2j + i N_2j+1, unweighted DIF of length h.
+    for (int j = threadIdx.x; j < H; j += NT) {
+        const uint32_t v0 = nn[2 * j], v1 = nn[2 * j + 1];
+        F2 z2; z2.re = v0; z2.im = v1;
+        uint32_t r0 = (v0 & P1) + (v0 >> 31), r1 = (v1 & P1) + (v1 >> 31);
+        F1 z1; z1.re = min(r0, r0 - P1); z1.im = min(r1, r1 - P1);
+        s2[swz(j)] = z2;
+        s1[swz(j)] = z1;
+    }
+    __syncthreads();
+    const F2* ht2 = tab2 + lt_half_off(M);
+    const F1* ht1 = tab1 + lt_half_off(M);
+    dif_unweighted<M - 1, NT>(s2, s1, ht2, ht1);
+    const F2* u2 = tab2 + lt_unpack_off(M);
+    const F1* u1 = tab1 + lt_unpack_off(M);
+    // half_nhat (cpu.rs:239-249) into elements h..2h.
+    for (int p = threadIdx.x; p < H; p += NT) {
+        const int q = p < 2 ? p : (3 << (31 - __clz(p))) - 1 - p;
+        {
+            const F2 zk = s2[swz(p)], zj = cconj(s2[swz(q)]);
+            const F2 e = cadd(zk, zj), wo = cmul(mul_mi(csub(zk, zj)), u2[p]);
+            const F2 xx = cadd(e, wo), yy = csub(e, wo);
+            s2[swz(H + p)] = p == 0 ? cadd(cmul(xx, inv8h2), mul_i(cmul(yy, inv8h2))) : cmul(xx, inv8h2);
+        }
+        {
+            const F1 zk = s1[swz(p)], zj = cconj(s1[swz(q)]);
+            const F1 e = cadd(zk, zj), wo = cmul(mul_mi(csub(zk, zj)), u1[p]);
+            const F1 xx = cadd(e, wo), yy = csub(e, wo);
+            s1[swz(H + p)] = p == 0 ? cadd(cmul(xx, inv8h1), mul_i(cmul(yy, inv8h1))) : cmul(xx, inv8h1);
+        }
+    }
+    __syncthreads();
+    // half_factors (cpu.rs:265-277): A at h-offset 0, B at h.
+    for (int p = threadIdx.x; p < H; p += NT) {
+        const int q = p < 2 ? p : (3 << (31 - __clz(p))) - 1 - p;
+        {
+            const F2 sp = s2[swz(H + p)], sq = s2[swz(H + q)];
+            const F2 nx = p == 0 ? f2(sp.re, 0) : sp, ny = p == 0 ? f2(sp.im, 0) : cconj(sq);
+            const F2 iu = u2[H + p], iiu = mul_i(iu);
+            const F2 X = cmul(nx, f2(add2(1, iiu.re), iiu.im)), Y = cmul(ny, f2(sub2(1, iiu.re), sub2(0, iiu.im)));
+            o2[N + p] = cadd(X, Y);
+            o2[N + H + p] = cmul(mul_mi(csub(X, Y)), u2[p]);
+        }
+        {
+            const F1 sp = s1[swz(H + p)], sq = s1[swz(H + q)];
+            const F1 nx = p == 0 ? f1(sp.re, 0) : sp, ny = p == 0 ? f1(sp.im, 0) : cconj(sq);
+            const F1 iu = u1[H + p], iiu = mul_i(iu);
+            const F1 X = cmul(nx, f1(add1(1, iiu.re), iiu.im)), Y = cmul(ny, f1(sub1(1, iiu.re), sub1(0, iiu.im)));
+            o1[N + p] = cadd(X, Y);
+            o1[N + H + p] = cmul(mul_mi(csub(X, Y)), u1[p]);
+        }
+    }
+}
+
+}  // namespace mm

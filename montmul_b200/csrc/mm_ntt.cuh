@@ -1,0 +1,331 @@
+// Shared-memory transforms of one vector per thread block: the reference's DIF and DIT
+// (montmul/src/cpu.rs:49-115) run as radix-8/4/2 passes, each pass = log2 R radix-2 stages done
+// in registers, one barrier per pass.
+//
+// Radix-R DIF pass with span q on the group b + j + k q (k < R): the R-point butterfly uses only
+// the fixed roots i and omega_8 (mm_field.cuh); the remaining factors of the R stages,
+// W^(j rev_R(k)) with W a primitive (R q)-th root, are applied to the outputs afterwards (they
+// commute with the later butterflies of the same pass). The DIT pass mirrors it: inputs first
+// multiplied by V^(j rev_R(k)), V = W^-1, then the inverse butterflies. Either way every
+// position ends with exactly the value the reference's radix-2 loops produce.
+//
+// Shared-memory layout: F2 array (16 B per element) then F1 array (8 B), element e stored at
+// swz(e). swz flips the low 3 bits by bits 3-5 and bit 3 by bit 6, which makes every radix-8 and
+// radix-4 pass free of bank conflicts in both arrays (checked by simulation over all spans).
+#pragma once
+#include "mm_field.cuh"
+
+namespace mm {
+
+__device__ __forceinline__ int swz(int e) {
+    return (e & ~15) | ((((e >> 3) ^ (e >> 6)) & 1) << 3) | ((e ^ (e >> 3)) & 7);
+}
+
+// ---- in-register butterflies (positions k of one group) ----
+// u + (-i) v and u - (-i) v
+__device__ __forceinline__ F1 cadd_mi(F1 u, F1 v) { return f1(add1(u.re, v.im), sub1(u.im, v.re)); }
+__device__ __forceinline__ F1 csub_mi2(F1 u, F1 v) { return f1(sub1(u.re, v.im), add1(u.im, v.re)); }
+__device__ __forceinline__ F2 cadd_mi(F2 u, F2 v) { return f2(add2(u.re, v.im), sub2(u.im, v.re)); }
+__device__ __forceinline__ F2 csub_mi2(F2 u, F2 v) { return f2(sub2(u.re, v.im), add2(u.im, v.re)); }
+
+template <int R, typename T> __device__ __forceinline__ void bf_dif(T* x);
+template <int R, typename T> __device__ __forceinline__ void bf_dit(T* x);
+
+template <> __device__ __forceinline__ void bf_dif<2, F1>(F1* x) { F1 u = x[0]; x[0] = cadd(u, x[1]); x[1] = csub(u, x[1]); }
+template <> __device__ __forceinline__ void bf_dif<2, F2>(F2* x) { F2 u = x[0]; x[0] = cadd(u, x[1]); x[1] = csub(u, x[1]); }
+template <> __device__ __forceinline__ void bf_dit<2, F1>(F1* x) { bf_dif<2, F1>(x); }
+template <> __device__ __forceinline__ void bf_dit<2, F2>(F2* x) { bf_dif<2, F2>(x); }
+
+template <typename T> __device__ __forceinline__ void bf_dif4(T* x) {
+    T a0 = cadd(x[0], x[2]), b0 = csub(x[0], x[2]);
+    T a1 = cadd(x[1], x[3]), b1 = csub_i(x[1], x[3]);
+    x[0] = cadd(a0, a1); x[1] = csub(a0, a1);
+    x[2] = cadd(b0, b1); x[3] = csub(b0, b1);
+}
+template <typename T> __device__ __forceinline__ void bf_dit4(T* x) {
+    T c0 = cadd(x[0], x[1]), c1 = csub(x[0], x[1]);
+    T c2 = cadd(x[2], x[3]), c3 = csub(x[2], x[3]);
+    x[0] = cadd(c0, c2); x[2] = csub(c0, c2);
+    x[1] = cadd_mi(c1, c3); x[3] = csub_mi2(c1, c3);
+}
+template <typename T> __device__ __forceinline__ void bf_dif8(T* x) {
+    T a0 = cadd(x[0], x[4]), b0 = csub(x[0], x[4]);
+    T a1 = cadd(x[1], x[5]), b1 = mul_w8(csub(x[1], x[5]));
+    T a2 = cadd(x[2], x[6]), b2 = csub_i(x[2], x[6]);
+    T a3 = cadd(x[3], x[7]), b3 = mul_w8(csub_i(x[3], x[7]));
+    T c0 = cadd(a0, a2), c2 = csub(a0, a2);
+    T c1 = cadd(a1, a3), c3 = csub_i(a1, a3);
+    T d0 = cadd(b0, b2), d2 = csub(b0, b2);
+    T d1 = cadd(b1, b3), d3 = csub_i(b1, b3);
+    x[0] = cadd(c0, c1); x[1] = csub(c0, c1);
+    x[2] = cadd(c2, c3); x[3] = csub(c2, c3);
+    x[4] = cadd(d0, d1); x[5] = csub(d0, d1);
+    x[6] = cadd(d2, d3); x[7] = csub(d2, d3);
+}
+template <typename T> __device__ __forceinline__ void bf_dit8(T* x) {
+    T c0 = cadd(x[0], x[1]), c1 = csub(x[0], x[1]);
+    T c2 = cadd(x[2], x[3]), c3 = csub(x[2], x[3]);
+    T c4 = cadd(x[4], x[5]), c5 = csub(x[4], x[5]);
+    T c6 = cadd(x[6], x[7]), c7 = csub(x[6], x[7]);
+    T a0 = cadd(c0, c2), a2 = csub(c0, c2);
+    T a1 = cadd_mi(c1, c3), a3 = csub_mi2(c1, c3);
+    T b0 = cadd(c4, c6), b2 = csub(c4, c6);
+    T b1 = cadd_mi(c5, c7), b3 = csub_mi2(c5, c7);
+    // stage with span 4: factors nu8^k on b_k, nu8 = omega_8^-1, nu8^2 = -i, nu8^3 = nu8 (-i)
+    T v1 = mul_v8(b1), v2 = mul_mi(b2), v3 = mul_mi(mul_v8(b3));
+    x[0] = cadd(a0, b0); x[4] = csub(a0, b0);
+    x[1] = cadd(a1, v1); x[5] = csub(a1, v1);
+    x[2] = cadd(a2, v2); x[6] = csub(a2, v2);
+    x[3] = cadd(a3, v3); x[7] = csub(a3, v3);
+}
+template <> __device__ __forceinline__ void bf_dif<4, F1>(F1* x) { bf_dif4(x); }
+template <> __device__ __forceinline__ void bf_dif<4, F2>(F2* x) { bf_dif4(x); }
+template <> __device__ __forceinline__ void bf_dit<4, F1>(F1* x) { bf_dit4(x); }
+template <> __device__ __forceinline__ void bf_dit<4, F2>(F2* x) { bf_dit4(x); }
+template <> __device__ __forceinline__ void bf_dif<8, F1>(F1* x) { bf_dif8(x); }
+template <> __device__ __forceinline__ void bf_dif<8, F2>(F2* x) { bf_dif8(x); }
+template <> __device__ __forceinline__ void bf_dit<8, F1>(F1* x) { bf_dit8(x); }
+template <> __device__ __forceinline__ void bf_dit<8, F2>(F2* x) { bf_dit8(x); }
+
+// ---- one unweighted pass over the shared vector ----
+// M = log2 of the transform length, I = pass index (DIF order), TAB = pointer to this
+// transform's table (F2 and F1 arrays with the same indices). No twiddles when q = 1.
+template <int M, int I, bool FWD, int NT, bool WEIGHTED>
+__device__ __forceinline__ void smem_pass(F2* s2, F1* s1, const F2* tab2, const F1* tab1) {
+    constexpr int R = sched_radix(M, I), Q = sched_q(M, I);
+    constexpr int G = (1 << M) / R;
+    constexpr int toff = FWD ? tab_fwd_off(M, I, WEIGHTED) : tab_inv_off(M, I, WEIGHTED);
+    for (int g = threadIdx.x; g < G; g += NT) {
+        const int j = g & (Q - 1);
+        const int b = (g / Q) * (R * Q) + j;
+        {
+            F2 x[R];
+#pragma unroll
+            for (int k = 0; k < R; ++k) x[k] = s2[swz(b + k * Q)];
+            if (FWD) {
+                bf_dif<R, F2>(x);
+                if (Q > 1) {
+#pragma unroll
+                    for (int k = 1; k < R; ++k) x[k] = cmul(x[k], tab2[toff + (k - 1) * Q + j]);
+                }
+            } else {
+                if (Q > 1) {
+#pragma unroll
+                    for (int k = 1; k < R; ++k) x[k] = cmul(x[k], tab2[toff + (k - 1) * Q + j]);
+                }
+                bf_dit<R, F2>(x);
+            }
+#pragma unroll
+            for (int k = 0; k < R; ++k) s2[swz(b + k * Q)] = x[k];
+        }
+        {
+            F1 x[R];
+#pragma unroll
+            for (int k = 0; k < R; ++k) x[k] = s1[swz(b + k * Q)];
+            if (FWD) {
+                bf_dif<R, F1>(x);
+                if (Q > 1) {
+#pragma unroll
+                    for (int k = 1; k < R; ++k) x[k] = cmul(x[k], tab1[toff + (k - 1) * Q + j]);
+                }
+            } else {
+                if (Q > 1) {
+#pragma unroll
+                    for (int k = 1; k < R; ++k) x[k] = cmul(x[k], tab1[toff + (k - 1) * Q + j]);
+                }
+                bf_dit<R, F1>(x);
+            }
+#pragma unroll
+            for (int k = 0; k < R; ++k) s1[swz(b + k * Q)] = x[k];
+        }
+    }
+    __syncthreads();
+}
+
+// ---- the weighted first DIF pass, straight from real limbs in global memory ----
+// Element j + k q of the input is (v, 0) with v the 32-bit limb (0 beyond `cnt`); its weight
+// zeta^(j + k q) = zeta^j zeta^(q k) splits into the pass constant zeta^(q k) on the input and
+// zeta^j folded into the output factors of the table.
+template <typename T> __device__ __forceinline__ T real_times(uint32_t v, T c);
+template <> __device__ __forceinline__ F1 real_times<F1>(uint32_t v, F1 c) {
+    uint32_t s = (v & P1) + (v >> 31);
+    s = min(s, s - P1);
+    return cmul_r(s, c);
+}
+template <> __device__ __forceinline__ F2 real_times<F2>(uint32_t v, F2 c) { return cmul_r((uint64_t)v, c); }
+
+template <int M, int NT>
+__device__ __forceinline__ void dif_first_from_limbs(const uint32_t* __restrict__ lim, int cnt, F2* s2, F1* s1,
+                                                     const F2* tab2, const F1* tab1) {
+    constexpr int R = sched_radix(M, 0), Q = sched_q(M, 0);
+    static_assert(Q > 1, "single-pass transforms use the fused pass");
+    constexpr int toff = tab_fwd_off(M, 0, true), coff = tab_in_const_off(M, true);
+    for (int j = threadIdx.x; j < Q; j += NT) {
+        uint32_t v[R];
+#pragma unroll
+        for (int k = 0; k < R; ++k) v[k] = (j + k * Q < cnt) ? lim[j + k * Q] : 0u;
+        {
+            F2 x[R];
+#pragma unroll
+            for (int k = 0; k < R; ++k) x[k] = real_times<F2>(v[k], tab2[coff + k]);
+            bf_dif<R, F2>(x);
+#pragma unroll
+            for (int k = 0; k < R; ++k) s2[swz(j + k * Q)] = cmul(x[k], tab2[toff + k * Q + j]);
+        }
+        {
+            F1 x[R];
+#pragma unroll
+            for (int k = 0; k < R; ++k) x[k] = real_times<F1>(v[k], tab1[coff + k]);
+            bf_dif<R, F1>(x);
+#pragma unroll
+            for (int k = 0; k < R; ++k) s1[swz(j + k * Q)] = cmul(x[k], tab1[toff + k * Q + j]);
+        }
+    }
+    __syncthreads();
+}
+
+// ---- the weighted last DIT pass: unweights by zeta^-(j + k q) / n into natural order ----
+// REAL_ONLY: only the real parts are needed (the low half of the product, coefficients < n).
+template <int M, int NT, bool REAL_ONLY>
+__device__ __forceinline__ void dit_last_weighted(F2* s2, F1* s1, const F2* tab2, const F1* tab1) {
+    constexpr int R = sched_radix(M, 0), Q = sched_q(M, 0);
+    static_assert(Q > 1, "single-pass transforms use the fused pass");
+    constexpr int toff = tab_inv_off(M, 0, true), coff = tab_out_const_off(M, true);
+    for (int j = threadIdx.x; j < Q; j += NT) {
+        {
+            F2 x[R];
+#pragma unroll
+            for (int k = 0; k < R; ++k) x[k] = cmul(s2[swz(j + k * Q)], tab2[toff + k * Q + j]);
+            bf_dit<R, F2>(x);
+#pragma unroll
+            for (int k = 0; k < R; ++k) {
+                if (REAL_ONLY) s2[swz(j + k * Q)].re = cmul_re(x[k], tab2[coff + k]);
+                else s2[swz(j + k * Q)] = cmul(x[k], tab2[coff + k]);
+            }
+        }
+        {
+            F1 x[R];
+#pragma unroll
+            for (int k = 0; k < R; ++k) x[k] = cmul(s1[swz(j + k * Q)], tab1[toff + k * Q + j]);
+            bf_dit<R, F1>(x);
+#pragma unroll
+            for (int k = 0; k < R; ++k) {
+                if (REAL_ONLY) s1[swz(j + k * Q)].re = cmul_re(x[k], tab1[coff + k]);
+                else s1[swz(j + k * Q)] = cmul(x[k], tab1[coff + k]);
+            }
+        }
+    }
+    __syncthreads();
+}
+
+// ---- the fused middle: last DIF pass (span 1), a pointwise operation, first DIT pass ----
+// OP::apply2/apply1(x, g) transforms the R spectrum values of group g (positions R g + k).
+// With a single pass (M <= 3) the same pass is also the weighted first/last pass.
+template <int M, int NT, bool REAL_ONLY, class OP>
+__device__ __forceinline__ void fused_mid(const uint32_t* __restrict__ lim, int cnt, F2* s2, F1* s1,
+                                          const F2* tab2, const F1* tab1, const OP& op) {
+    constexpr int P = sched_passes(M);
+    constexpr int R = sched_radix(M, P - 1);
+    constexpr int G = (1 << M) / R;
+    constexpr bool single = (P == 1);
+    constexpr int cin = tab_in_const_off(M, true), cout = tab_out_const_off(M, true);
+    for (int g = threadIdx.x; g < G; g += NT) {
+        {
+            F2 x[R];
+            if (single) {
+#pragma unroll
+                for (int k = 0; k < R; ++k) x[k] = real_times<F2>(k < cnt ? lim[k] : 0u, tab2[cin + k]);
+            } else {
+#pragma unroll
+                for (int k = 0; k < R; ++k) x[k] = s2[swz(R * g + k)];
+            }
+            bf_dif<R, F2>(x);
+            if (!op.template apply2<R>(x, g)) {
+                bf_dit<R, F2>(x);
+#pragma unroll
+                for (int k = 0; k < R; ++k) {
+                    if (single) {
+                        if (REAL_ONLY) s2[k].re = cmul_re(x[k], tab2[cout + k]);
+                        else s2[k] = cmul(x[k], tab2[cout + k]);
+                    } else {
+                        s2[swz(R * g + k)] = x[k];
+                    }
+                }
+            }
+        }
+        {
+            F1 x[R];
+            if (single) {
+#pragma unroll
+                for (int k = 0; k < R; ++k) x[k] = real_times<F1>(k < cnt ? lim[k] : 0u, tab1[cin + k]);
+            } else {
+#pragma unroll
+                for (int k = 0; k < R; ++k) x[k] = s1[swz(R * g + k)];
+            }
+            bf_dif<R, F1>(x);
+            if (!op.template apply1<R>(x, g)) {
+                bf_dit<R, F1>(x);
+#pragma unroll
+                for (int k = 0; k < R; ++k) {
+                    if (single) {
+                        if (REAL_ONLY) s1[k].re = cmul_re(x[k], tab1[cout + k]);
+                        else s1[k] = cmul(x[k], tab1[cout + k]);
+                    } else {
+                        s1[swz(R * g + k)] = x[k];
+                    }
+                }
+            }
+        }
+    }
+    __syncthreads();
+}
+
+// ---- whole transforms ----
+// Forward weighted transform of real limbs up to (not including) the last pass.
+template <int M, int NT>
+__device__ __forceinline__ void fwd_limbs(const uint32_t* __restrict__ lim, int cnt, F2* s2, F1* s1,
+                                          const F2* t2, const F1* t1) {
+    constexpr int P = sched_passes(M);
+    if constexpr (P >= 2) {
+        dif_first_from_limbs<M, NT>(lim, cnt, s2, s1, t2, t1);
+        if constexpr (P >= 3) smem_pass<M, 1, true, NT, true>(s2, s1, t2, t1);
+        if constexpr (P >= 4) smem_pass<M, 2, true, NT, true>(s2, s1, t2, t1);
+        if constexpr (P >= 5) smem_pass<M, 3, true, NT, true>(s2, s1, t2, t1);
+        static_assert(P <= 5, "schedule longer than the shared-memory lengths need");
+    }
+}
+
+// Inverse weighted transform from after the fused pass down to natural order.
+template <int M, int NT, bool REAL_ONLY>
+__device__ __forceinline__ void inv_to_natural(F2* s2, F1* s1, const F2* t2, const F1* t1) {
+    constexpr int P = sched_passes(M);
+    if constexpr (P >= 2) {
+        if constexpr (P >= 5) smem_pass<M, 3, false, NT, true>(s2, s1, t2, t1);
+        if constexpr (P >= 4) smem_pass<M, 2, false, NT, true>(s2, s1, t2, t1);
+        if constexpr (P >= 3) smem_pass<M, 1, false, NT, true>(s2, s1, t2, t1);
+        dit_last_weighted<M, NT, REAL_ONLY>(s2, s1, t2, t1);
+    }
+}
+
+// Unweighted transforms of the first 2^M elements (the wraparound path's length h), all in smem.
+template <int M, int NT>
+__device__ __forceinline__ void dif_unweighted(F2* s2, F1* s1, const F2* t2, const F1* t1) {
+    constexpr int P = sched_passes(M);
+    smem_pass<M, 0, true, NT, false>(s2, s1, t2, t1);
+    if constexpr (P >= 2) smem_pass<M, 1, true, NT, false>(s2, s1, t2, t1);
+    if constexpr (P >= 3) smem_pass<M, 2, true, NT, false>(s2, s1, t2, t1);
+    if constexpr (P >= 4) smem_pass<M, 3, true, NT, false>(s2, s1, t2, t1);
+    if constexpr (P >= 5) smem_pass<M, 4, true, NT, false>(s2, s1, t2, t1);
+    static_assert(P <= 5, "schedule longer than the shared-memory lengths need");
+}
+template <int M, int NT>
+__device__ __forceinline__ void dit_unweighted(F2* s2, F1* s1, const F2* t2, const F1* t1) {
+    constexpr int P = sched_passes(M);
+    if constexpr (P >= 5) smem_pass<M, 4, false, NT, false>(s2, s1, t2, t1);
+    if constexpr (P >= 4) smem_pass<M, 3, false, NT, false>(s2, s1, t2, t1);
+    if constexpr (P >= 3) smem_pass<M, 2, false, NT, false>(s2, s1, t2, t1);
+    if constexpr (P >= 2) smem_pass<M, 1, false, NT, false>(s2, s1, t2, t1);
+    smem_pass<M, 0, false, NT, false>(s2, s1, t2, t1);
+}
+
+}  // namespace mm
