@@ -97,10 +97,18 @@ void mm_b200_destroy(mm_b200_batch *b);
  * returns; mm_b200_sync waits and performs run's error check. mm_b200_stream is the
  * cudaStream_t the batch launches on. */
 int mm_b200_run_async(mm_b200_batch *b, size_t bits);
+/* Uploads pending loads and exponents now (run does this itself before its first launch). */
+int mm_b200_push(mm_b200_batch *b);
 int mm_b200_sync(mm_b200_batch *b);
 void *mm_b200_stream(mm_b200_batch *b);
 /* Kernel launches issued by this batch so far (for launch accounting). */
 uint64_t mm_b200_launches(const mm_b200_batch *b);
+
+/* Integer roofline probe (no counterpart in the reference, whose roofline is not measured):
+ * the peak rate of butterfly pairs (a GF(p^2) product, an add and a sub in both fields) of the
+ * kernels' arithmetic from register-resident chains on every SM of `device`; `iters` chain
+ * steps per thread. Writes pairs per second and the timed kernel's milliseconds. */
+int mm_b200_bfly_peak(int device, int iters, double *pairs_per_s, double *ms);
 
 #ifdef __cplusplus
 }

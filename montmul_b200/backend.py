@@ -57,8 +57,10 @@ SIGNATURES = {
     "mm_b200_destroy": ([_vp], None),
     "mm_b200_run_async": ([_vp, _sz], C.c_int),
     "mm_b200_sync": ([_vp], C.c_int),
+    "mm_b200_push": ([_vp], C.c_int),
     "mm_b200_stream": ([_vp], _vp),
     "mm_b200_launches": ([_vp], C.c_uint64),
+    "mm_b200_bfly_peak": ([C.c_int, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)], C.c_int),
 }
 
 _lib = None
@@ -77,6 +79,13 @@ def lib():
             f.restype = res
         _lib = L
     return _lib
+
+
+def bfly_peak(device: int = 0, iters: int = 1 << 14):
+    """(butterfly pairs per second, kernel ms) of the integer roofline probe."""
+    r, ms = C.c_double(), C.c_double()
+    _check(lib().mm_b200_bfly_peak(device, iters, C.byref(r), C.byref(ms)))
+    return r.value, ms.value
 
 
 def _check(rc: int) -> None:
@@ -167,6 +176,9 @@ class B200:
 
     def run_async(self, st, bits):
         _check(lib().mm_b200_run_async(st.ptr, bits))
+
+    def push(self, st):
+        _check(lib().mm_b200_push(st.ptr))
 
     def sync(self, st):
         _check(lib().mm_b200_sync(st.ptr))

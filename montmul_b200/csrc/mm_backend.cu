@@ -96,7 +96,10 @@ struct mm_b200_batch {
     F1* d_spec1 = nullptr;
     size_t ew = 0, exp_cap = 0;
     const DevTables* tab = nullptr;
-    std::vector<uint32_t> host_x;
+    uint32_t* host_x = nullptr;    // pinned, slots x k
+    size_t host_x_len = 0;
+    uint32_t* host_exp = nullptr;  // pinned staging of the exponent words, nbits and pos
+    size_t host_exp_cap = 0;
     bool host_x_valid = true;
     bool device_x_stale = false;
     std::vector<std::vector<uint32_t>> exps;
@@ -155,7 +158,7 @@ SlotArgs slot_args(const mm_b200_batch* b) {
 
 int pull_x(mm_b200_batch* b) {
     if (b->host_x_valid) return MM_OK;
-    MM_CK(cudaMemcpyAsync(b->host_x.data(), b->d_x, b->host_x.size() * 4, cudaMemcpyDeviceToHost, b->stream));
+    MM_CK(cudaMemcpyAsync(b->host_x, b->d_x, b->host_x_len * 4, cudaMemcpyDeviceToHost, b->stream));
     MM_CK(cudaStreamSynchronize(b->stream));
     b->host_x_valid = true;
     return MM_OK;
@@ -164,25 +167,36 @@ int pull_x(mm_b200_batch* b) {
 // Uploads host-side changes (loaded values, exponents) before a launch (gpu/mod.rs:161-176).
 int push(mm_b200_batch* b) {
     if (b->device_x_stale) {
-        MM_CK(cudaMemcpyAsync(b->d_x, b->host_x.data(), b->host_x.size() * 4, cudaMemcpyHostToDevice, b->stream));
+        MM_CK(cudaMemcpyAsync(b->d_x, b->host_x, b->host_x_len * 4, cudaMemcpyHostToDevice, b->stream));
         b->device_x_stale = false;
     }
     if (b->exp_dirty) {
         size_t ew = 1;
         for (auto& e : b->exps) ew = std::max(ew, e.size());
-        std::vector<uint32_t> words(b->slots * ew, 0);
+        // The staging buffer may still feed a copy of the previous push.
+        MM_CK(cudaStreamSynchronize(b->stream));
+        const size_t need = b->slots * (ew + 2);
+        if (need > b->host_exp_cap) {
+            if (b->host_exp) MM_CK(cudaFreeHost(b->host_exp));
+            b->host_exp = nullptr;
+            MM_CK(cudaMallocHost(&b->host_exp, need * 4));
+            b->host_exp_cap = need;
+        }
+        uint32_t* words = b->host_exp;
+        std::memset(words, 0, b->slots * ew * 4);
         for (size_t i = 0; i < b->slots; ++i)
-            std::copy(b->exps[i].begin(), b->exps[i].end(), words.begin() + i * ew);
+            std::copy(b->exps[i].begin(), b->exps[i].end(), words + i * ew);
+        std::memcpy(words + b->slots * ew, b->nbits.data(), b->slots * 4);
+        std::memcpy(words + b->slots * (ew + 1), b->pos.data(), b->slots * 4);
         if (ew > b->exp_cap) {
             if (b->d_exp) MM_CK(cudaFree(b->d_exp));
             MM_CK(cudaMalloc(&b->d_exp, b->slots * ew * 4));
             b->exp_cap = ew;
         }
         b->ew = ew;
-        MM_CK(cudaMemcpyAsync(b->d_exp, words.data(), words.size() * 4, cudaMemcpyHostToDevice, b->stream));
-        MM_CK(cudaMemcpyAsync(b->d_nbits, b->nbits.data(), b->slots * 4, cudaMemcpyHostToDevice, b->stream));
-        MM_CK(cudaMemcpyAsync(b->d_pos, b->pos.data(), b->slots * 4, cudaMemcpyHostToDevice, b->stream));
-        MM_CK(cudaStreamSynchronize(b->stream));
+        MM_CK(cudaMemcpyAsync(b->d_exp, words, b->slots * ew * 4, cudaMemcpyHostToDevice, b->stream));
+        MM_CK(cudaMemcpyAsync(b->d_nbits, words + b->slots * ew, b->slots * 4, cudaMemcpyHostToDevice, b->stream));
+        MM_CK(cudaMemcpyAsync(b->d_pos, words + b->slots * (ew + 1), b->slots * 4, cudaMemcpyHostToDevice, b->stream));
         b->exp_dirty = false;
     }
     return MM_OK;
@@ -363,7 +377,9 @@ int mm_b200_create(mm_b200_device* dev, size_t k, size_t len, uint32_t base, siz
     MM_CK(cudaStreamSynchronize(b->stream));
     MM_CK(cudaFree(d_n));
     MM_CK(cudaFree(d_np));
-    b->host_x.assign(slots * k, 0);
+    MM_CK(cudaMallocHost(&b->host_x, slots * k * 4));
+    b->host_x_len = slots * k;
+    std::memset(b->host_x, 0, slots * k * 4);
     b->host_x_valid = true;
     b->device_x_stale = false;
     b->exps.assign(slots, std::vector<uint32_t>());
@@ -377,14 +393,16 @@ int mm_b200_load(mm_b200_batch* b, size_t i, const uint32_t* limbs) {
     if (!b || !limbs || i >= b->slots) return fail(MM_ERR_ARG, "load: bad slot");
     int rc = pull_x(b);
     if (rc) return rc;
-    std::memcpy(b->host_x.data() + i * b->k, limbs, b->k * 4);
+    std::memcpy(b->host_x + i * b->k, limbs, b->k * 4);
     b->device_x_stale = true;
     return MM_OK;
 }
 
 int mm_b200_load_all(mm_b200_batch* b, const uint32_t* limbs) {
     if (!b || !limbs) return fail(MM_ERR_ARG, "load_all: null argument");
-    std::memcpy(b->host_x.data(), limbs, b->host_x.size() * 4);
+    // The pinned buffer may still feed the upload of a previous push.
+    MM_CK(cudaStreamSynchronize(b->stream));
+    std::memcpy(b->host_x, limbs, b->host_x_len * 4);
     b->host_x_valid = true;
     b->device_x_stale = true;
     return MM_OK;
@@ -418,6 +436,12 @@ int mm_b200_run_async(mm_b200_batch* b, size_t bits) {
     return launch_steps(b, bits);
 }
 
+int mm_b200_push(mm_b200_batch* b) {
+    if (!b) return fail(MM_ERR_ARG, "push: null batch");
+    MM_CK(cudaSetDevice(b->dev->device));
+    return push(b);
+}
+
 int mm_b200_sync(mm_b200_batch* b) {
     if (!b) return fail(MM_ERR_ARG, "sync: null batch");
     MM_CK(cudaStreamSynchronize(b->stream));
@@ -448,7 +472,7 @@ int mm_b200_read(mm_b200_batch* b, size_t i, uint32_t* limbs) {
     if (!b || !limbs || i >= b->slots) return fail(MM_ERR_ARG, "read: bad slot");
     int rc = pull_x(b);
     if (rc) return rc;
-    std::memcpy(limbs, b->host_x.data() + i * b->k, b->k * 4);
+    std::memcpy(limbs, b->host_x + i * b->k, b->k * 4);
     return MM_OK;
 }
 
@@ -456,7 +480,7 @@ int mm_b200_read_all(mm_b200_batch* b, uint32_t* limbs) {
     if (!b || !limbs) return fail(MM_ERR_ARG, "read_all: null argument");
     int rc = pull_x(b);
     if (rc) return rc;
-    std::memcpy(limbs, b->host_x.data(), b->host_x.size() * 4);
+    std::memcpy(limbs, b->host_x, b->host_x_len * 4);
     return MM_OK;
 }
 
@@ -486,6 +510,8 @@ void mm_b200_destroy(mm_b200_batch* b) {
     cudaFree(b->d_spec2);
     cudaFree(b->d_spec1);
     if (b->stream) cudaStreamDestroy(b->stream);
+    if (b->host_x) cudaFreeHost(b->host_x);
+    if (b->host_exp) cudaFreeHost(b->host_exp);
     delete b;
 }
 

@@ -106,7 +106,8 @@ def test_oversized_batch_is_error(gpu):
     from montmul_b200.backend import lib
     dev = gpu()
     k, length = 8192, 16384
-    slots = dev.free_memory() // lib().mm_b200_batch_bytes(1, length, 1) * 11 // 10 + 1
+    per_slot = lib().mm_b200_batch_bytes(2, length, 1) - lib().mm_b200_batch_bytes(1, length, 1)
+    slots = dev.free_memory() // per_slot * 11 // 10 + 1
     assert lib().mm_b200_batch_bytes(slots, length, 1) > dev.free_memory()
     row = np.zeros((1, k), np.uint32)
     ptr = C.c_void_p()
