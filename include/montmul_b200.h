@@ -104,6 +104,22 @@ void *mm_b200_stream(mm_b200_batch *b);
 /* Kernel launches issued by this batch so far (for launch accounting). */
 uint64_t mm_b200_launches(const mm_b200_batch *b);
 
+/* a b R^-1 mod N (lazy, in [0, 2N)) for slot `slot`'s modulus N, without allocating: no
+ * counterpart in the reference. For callers that cannot allocate device memory at the point of
+ * the call: code under CUDA stream capture (cudaMalloc/cudaFree cannot be captured), services
+ * whose device memory belongs to their own pool allocator, loops that cannot afford cudaFree's
+ * implicit device synchronization. d_a, d_b (inputs) and d_out (output) are device buffers of k
+ * limbs the caller owns; d_err (optional) receives 0, or 1 when a carry that must vanish did
+ * not. The work is enqueued on `stream` (a cudaStream_t; NULL is the legacy default stream)
+ * and the call returns without waiting. Intermediates live in a static 256 KiB device array
+ * that every GPU loading this library holds until exit; lengths needing more scratch are
+ * rejected with MM_ERR_ARG (every length this library builds fits). The first call on each
+ * device looks up that array's device address and sets kernel attributes, so make it before
+ * any stream capture. All calls share the array: calls that overlap on the GPU race and must
+ * be serialized by the caller. */
+int mm_b200_mul_noalloc(const mm_b200_batch *b, size_t slot, const uint32_t *d_a, const uint32_t *d_b,
+                        uint32_t *d_out, uint32_t *d_err, void *stream);
+
 /* Integer roofline probe (no counterpart in the reference, whose roofline is not measured):
  * the peak rate of butterfly pairs (a GF(p^2) product, an add and a sub in both fields) of the
  * kernels' arithmetic from register-resident chains on every SM of `device`; `iters` chain

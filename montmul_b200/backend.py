@@ -60,6 +60,7 @@ SIGNATURES = {
     "mm_b200_push": ([_vp], C.c_int),
     "mm_b200_stream": ([_vp], _vp),
     "mm_b200_launches": ([_vp], C.c_uint64),
+    "mm_b200_mul_noalloc": ([_vp, _sz, _vp, _vp, _vp, _vp, _vp], C.c_int),
     "mm_b200_bfly_peak": ([C.c_int, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)], C.c_int),
 }
 

@@ -240,6 +240,21 @@ int launch_steps(mm_b200_batch* b, size_t bits) {
 
 }  // namespace
 
+// Accessors for entry points defined in other translation units.
+int mm_set_error(int code, const std::string& msg) { return fail(code, msg); }
+
+int mm_batch_view(const mm_b200_batch* b, int* device, int* m, const F2** c2, const F1** c1, const F2** tab2,
+                  const F1** tab1, size_t* slots) {
+    *device = b->dev->device;
+    *m = b->m;
+    *c2 = b->d_c2;
+    *c1 = b->d_c1;
+    *tab2 = b->tab->t2;
+    *tab1 = b->tab->t1;
+    *slots = b->slots;
+    return MM_OK;
+}
+
 extern "C" {
 
 const char* mm_b200_last_error(void) { return g_err.c_str(); }

@@ -28,6 +28,9 @@ struct __align__(16) F2 { uint64_t re, im; };
 constexpr int kMaxSharedLogN = 13;
 constexpr int kMinLogN = 2;   // L = 8
 
+// Dynamic shared memory of one block at length 2^(m+1): F2 vector (16 n B), F1 vector (8 n B).
+MM_HD constexpr int smem_bytes_host(int m) { return 24 << m; }
+
 // ---- pass schedule: radices, DIF order ----
 // m = log2 n. m = 3a -> [8]*a; m = 3a + 1 -> [4, 4, 8*(a-1)]; m = 3a + 2 -> [4, 8*a];
 // m = 1 -> [2], m = 2 -> [4]. Radix-8 passes dominate; the last DIF pass (span 1) carries no
