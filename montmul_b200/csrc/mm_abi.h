@@ -16,7 +16,7 @@ struct SlotArgs {
     const uint32_t* nbits;
     uint32_t* pos;
     uint32_t* err;        // set to 1 when a carry that must vanish does not
-    const F2* tab2;       // this length's tables (mm_common.h layout)
+    const F2K* tab2;      // this length's tables (mm_common.h layout; M61 twiddles in Karatsuba form)
     const F1* tab1;
     uint32_t ew;
     uint32_t base;
@@ -24,7 +24,7 @@ struct SlotArgs {
 
 typedef void (*StepFn)(SlotArgs, uint32_t, uint32_t);
 typedef void (*MulFn)(SlotArgs, uint32_t, uint32_t, uint32_t, F2*, F1*);
-typedef void (*SetupFn)(const uint32_t*, const uint32_t*, F2*, F1*, const F2*, const F1*, F2, F1, uint32_t);
+typedef void (*SetupFn)(const uint32_t*, const uint32_t*, F2*, F1*, const F2K*, const F1*, F2, F1, uint32_t);
 
 struct KernelSet {
     StepFn step;

@@ -52,7 +52,7 @@ bool kernel_set(int m, KernelSet& ks) {
 }
 
 struct DevTables {
-    F2* t2 = nullptr;
+    F2K* t2 = nullptr;
     F1* t1 = nullptr;
     F2 inv8h2;
     F1 inv8h1;
@@ -114,12 +114,12 @@ int ensure_tables(mm_b200_device* dev, int m, const DevTables** out) {
     std::lock_guard<std::mutex> lock(dev->mu);
     auto it = dev->tables.find(m);
     if (it == dev->tables.end()) {
-        std::vector<F2> t2 = host::gen_length_tables<F2>(m);
+        std::vector<F2K> t2 = host::karatsuba_form(host::gen_length_tables<F2>(m));
         std::vector<F1> t1 = host::gen_length_tables<F1>(m);
         DevTables d;
-        MM_CK(cudaMalloc(&d.t2, t2.size() * sizeof(F2)));
+        MM_CK(cudaMalloc(&d.t2, t2.size() * sizeof(F2K)));
         MM_CK(cudaMalloc(&d.t1, t1.size() * sizeof(F1)));
-        MM_CK(cudaMemcpy(d.t2, t2.data(), t2.size() * sizeof(F2), cudaMemcpyHostToDevice));
+        MM_CK(cudaMemcpy(d.t2, t2.data(), t2.size() * sizeof(F2K), cudaMemcpyHostToDevice));
         MM_CK(cudaMemcpy(d.t1, t1.data(), t1.size() * sizeof(F1), cudaMemcpyHostToDevice));
         d.inv8h2 = host::inv8h<F2>(m);
         d.inv8h1 = host::inv8h<F1>(m);
@@ -243,7 +243,7 @@ int launch_steps(mm_b200_batch* b, size_t bits) {
 // Accessors for entry points defined in other translation units.
 int mm_set_error(int code, const std::string& msg) { return fail(code, msg); }
 
-int mm_batch_view(const mm_b200_batch* b, int* device, int* m, const F2** c2, const F1** c1, const F2** tab2,
+int mm_batch_view(const mm_b200_batch* b, int* device, int* m, const F2** c2, const F1** c1, const F2K** tab2,
                   const F1** tab1, size_t* slots) {
     *device = b->dev->device;
     *m = b->m;
@@ -327,7 +327,7 @@ size_t mm_b200_batch_bytes(size_t slots, size_t len, size_t exp_words) {
     // pos and err, per slot; plus mul's spectrum scratch (24n) and this length's tables.
     const size_t per_slot = 4 * n + 8 * n + 48 * n + 4 * exp_words + 12;
     const int m = log2_exact(n);
-    const size_t tabs = m >= kMinLogN ? (size_t)lt_size(m) * 24 : 0;
+    const size_t tabs = m >= kMinLogN ? (size_t)lt_size(m) * (sizeof(F2K) + sizeof(F1)) : 0;
     return slots * per_slot + 24 * n + tabs;
 }
 

@@ -91,7 +91,7 @@ struct Acc96 {
 // is re of element q, q >= n is im of element q - n), written to `out` (2n limbs, global).
 // Returns the carry out of the top, which must be 0 for a product that fits.
 template <int M, int NT>
-__device__ __forceinline__ uint64_t carry_product(const F2* s2, const F1* s1, uint32_t* __restrict__ out, uint64_t* sc) {
+__device__ __noinline__ uint64_t carry_product(const F2* s2, const F1* s1, uint32_t* __restrict__ out, uint64_t* sc) {
     constexpr int N = 1 << M, COUNT = 2 * N;
     constexpr int E = cmax(2, COUNT / NT), TA = COUNT / E;
     const int t = threadIdx.x;
@@ -127,7 +127,7 @@ __device__ __forceinline__ uint64_t carry_product(const F2* s2, const F1* s1, ui
 // m = low n limbs of the product in natural order (coefficients q < n: re of element q), then
 // packed in place for the wraparound path as z_j = m_2j + i m_2j+1, j < n/2 (cpu.rs:286-295).
 template <int M, int NT>
-__device__ __forceinline__ void carry_low_and_pack(F2* s2, F1* s1, uint64_t* sc) {
+__device__ __noinline__ void carry_low_and_pack(F2* s2, F1* s1, uint64_t* sc) {
     constexpr int N = 1 << M, COUNT = N;
     constexpr int E = cmax(2, COUNT / NT), TA = COUNT / E;
     const int t = threadIdx.x;
@@ -167,7 +167,7 @@ __device__ __forceinline__ void carry_low_and_pack(F2* s2, F1* s1, uint64_t* sc)
 // T (2n limbs) in global memory; writes x (n limbs). cpu.rs:297-328. Returns false when the
 // final carry out is not 0 (a product that did not fit).
 template <int M, int NT>
-__device__ __forceinline__ bool wrap_combine(const F2* s2, const F1* s1, const uint32_t* __restrict__ tl,
+__device__ __noinline__ bool wrap_combine(const F2* s2, const F1* s1, const uint32_t* __restrict__ tl,
                                              uint32_t* __restrict__ x, uint64_t* sc) {
     constexpr int K = 1 << M, COUNT = K;
     constexpr int E = cmax(2, COUNT / NT), TA = COUNT / E;

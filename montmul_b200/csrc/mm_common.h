@@ -22,6 +22,8 @@ constexpr uint64_t P2 = 0x1fffffffffffffffull;   // M61
 
 struct __align__(8) F1 { uint32_t re, im; };
 struct __align__(16) F2 { uint64_t re, im; };
+// A GF(M61^2) twiddle in the form the Karatsuba product reads: re, im, re + im, im - re (mod p).
+struct __align__(16) F2K { uint64_t re, im, s, d; };
 
 // Largest transform length handled with the whole vector in shared memory: n = 8192
 // (L = 16384) needs 24 n = 196,608 B of the 227 KB a B200 block may opt into.

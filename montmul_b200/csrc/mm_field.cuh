@@ -128,10 +128,73 @@ __device__ __forceinline__ F2 mul_v8(F2 x) { return f2(rot2(add2(x.re, x.im)), r
 __device__ __forceinline__ F2 mul_i(F2 x) { return f2(sub2(0, x.im), x.re); }
 __device__ __forceinline__ F2 mul_mi(F2 x) { return f2(x.im, sub2(0, x.re)); }
 
+// ---- lazy GF(M61) and GF(M61^2) ----
+// Values are kept below 2^64 instead of below p; a value is "reduced" when it is below
+// ONE = 2^61 + 2^34, the invariant of everything stored between passes. Sums are not reduced;
+// a difference a - b becomes a + (K p - b) with K p at least b's bound; lfold brings any u64
+// below 2^61 + 8. The radix-8/4/2 butterflies fold where their bounds would pass 2^64; an
+// interval model of every operation checks the bounds. Canonical form (lcanon) is needed only
+// where the value leaves the transform domain (CRT) or becomes a multiplier constant.
+__device__ __forceinline__ uint64_t lfold(uint64_t x) { return (x & P2) + (x >> 61); }
+__device__ __forceinline__ uint64_t lcanon(uint64_t x) {
+    uint64_t s = lfold(x);
+    return min(s, s - P2);
+}
+template <int K> __device__ __forceinline__ uint64_t lsub(uint64_t a, uint64_t b) { return a + ((uint64_t)K * P2 - b); }
+// x 2^30 mod p for any u64 x, below 2^61 + 2^33.
+__device__ __forceinline__ uint64_t lrot(uint64_t x) { return ((x << 30) & P2) + (x >> 31); }
+// a b mod p below p + (a b >> 61) for a b < 2^125 (one fold of the 128-bit product).
+__device__ __forceinline__ uint64_t lmul1(uint64_t a, uint64_t b) {
+    uint64_t lo = a * b, hi = __umul64hi(a, b);
+    return (lo & P2) + ((hi << 3) | (lo >> 61));
+}
+__device__ __forceinline__ F2 lcfold(F2 x) { return f2(lfold(x.re), lfold(x.im)); }
+__device__ __forceinline__ F2 lccanon(F2 x) { return f2(lcanon(x.re), lcanon(x.im)); }
+__device__ __forceinline__ F2 lcadd(F2 a, F2 b) { return f2(a.re + b.re, a.im + b.im); }
+template <int K> __device__ __forceinline__ F2 lcsub(F2 a, F2 b) { return f2(lsub<K>(a.re, b.re), lsub<K>(a.im, b.im)); }
+// (a - b) i
+template <int K> __device__ __forceinline__ F2 lcsub_i(F2 a, F2 b) { return f2(lsub<K>(b.im, a.im), lsub<K>(a.re, b.re)); }
+// u + (-i) v and u - (-i) v
+template <int K> __device__ __forceinline__ F2 lcadd_mi(F2 u, F2 v) { return f2(u.re + v.im, lsub<K>(u.im, v.re)); }
+template <int K> __device__ __forceinline__ F2 lcsub_mi(F2 u, F2 v) { return f2(lsub<K>(u.re, v.im), u.im + v.re); }
+// x omega_8 = x (1 + i) 2^30 and x omega_8^-1 = x (1 - i) 2^30, reduced outputs
+template <int K> __device__ __forceinline__ F2 lw8(F2 x) { return f2(lrot(lsub<K>(x.re, x.im)), lrot(x.re + x.im)); }
+template <int K> __device__ __forceinline__ F2 lv8(F2 x) { return f2(lrot(x.re + x.im), lrot(lsub<K>(x.im, x.re))); }
+// x (-i)
+template <int K> __device__ __forceinline__ F2 lmi(F2 x) { return f2(x.im, lsub<K>(0, x.re)); }
+// x w for reduced x and a twiddle in Karatsuba form: k1 = wr (xr + xi), k2 = xr (wi - wr),
+// k3 = xi (wr + wi); re = k1 - k3, im = k1 + k2. Three products instead of four.
+__device__ __forceinline__ F2 lkmul(F2 x, const F2K& w) {
+    const uint64_t k1 = lmul1(x.re + x.im, w.re), k2 = lmul1(x.re, w.d), k3 = lmul1(x.im, w.s);
+    return f2(lfold(lsub<3>(k1, k3)), lfold(k1 + k2));
+}
+// x w for reduced x and a canonical constant w (its Karatsuba sums formed here).
+__device__ __forceinline__ F2 lkmulc(F2 x, F2 w) {
+    const uint64_t s = w.re + w.im, d = lsub<1>(w.im, w.re);
+    const uint64_t k1 = lmul1(x.re + x.im, w.re), k2 = lmul1(x.re, d), k3 = lmul1(x.im, s);
+    return f2(lfold(lsub<4>(k1, k3)), lfold(k1 + k2));
+}
+// re(x w) for reduced x and a Karatsuba-form twiddle.
+__device__ __forceinline__ uint64_t lkmul_re(F2 x, const F2K& w) {
+    return lfold(lmul1(x.re, w.re) + lmul1(x.im, P2 - w.im));
+}
+// real 32-bit limb times a canonical constant, reduced.
+__device__ __forceinline__ F2 lreal_times(uint32_t v, const F2K& c) { return f2(lfold(lmul1(v, c.re)), lfold(lmul1(v, c.im))); }
+// x^2 c for reduced x and c <= 4, reduced.
+__device__ __forceinline__ F2 lsqr_scale(F2 x, uint32_t c) {
+    const uint64_t re = lfold(lmul1(x.re + x.im, lsub<2>(x.re, x.im)));
+    const uint64_t t = lmul1(x.re, x.im);
+    const uint64_t im = lfold(t + t);
+    if (c == 1) return f2(re, im);
+    return f2(lfold(re * c), lfold(im * c));
+}
+
 // ---- CRT (field.rs:288-294) ----
 // The unique C < M31 * M61 with C = c1 mod M31 and C = c2 mod M61, as three 32-bit words.
 // (M61 mod M31)^-1 = -2 mod M31, so h = 2 (c2 mod M31 - c1) mod M31 and C = c2 + M61 h.
+// c2 may be any reduced (lazy) M61 value; it is made canonical first.
 __device__ __forceinline__ void crt3(uint32_t c1, uint64_t c2, uint32_t& w0, uint32_t& w1, uint32_t& w2) {
+    c2 = lcanon(c2);
     uint32_t c2m = (uint32_t)(c2 & P1) + (uint32_t)(c2 >> 31);   // < 2^31 + 2^30
     c2m = min(c2m, c2m - P1);
     uint32_t h = dbl1(sub1(c2m, c1));

@@ -150,6 +150,14 @@ template <class E> inline std::vector<E> gen_length_tables(int m) {
     return t;
 }
 
+// M61 tables as the device's Karatsuba products read them: (re, im, re + im, im - re) mod p.
+inline std::vector<F2K> karatsuba_form(const std::vector<F2>& t) {
+    std::vector<F2K> out(t.size());
+    for (size_t i = 0; i < t.size(); ++i)
+        out[i] = F2K{t[i].re, t[i].im, add2(t[i].re, t[i].im), sub2(t[i].im, t[i].re)};
+    return out;
+}
+
 // (8 h)^-1 with h = n/2 = 2^(m-1) (cpu.rs:243).
 template <class E> inline E inv8h(int m) { return Gf<E>::inv(Gf<E>::from((uint64_t)8 << (m - 1))); }
 

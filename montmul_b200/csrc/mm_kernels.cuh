@@ -20,7 +20,7 @@ struct SquareOp {
     uint32_t c;
     template <int R> __device__ __forceinline__ bool apply2(F2* x, int) const {
 #pragma unroll
-        for (int k = 0; k < R; ++k) { x[k] = csqr(x[k]); if (c != 1) x[k] = cscale(x[k], c); }
+        for (int k = 0; k < R; ++k) x[k] = lsqr_scale(x[k], c);
         return false;
     }
     template <int R> __device__ __forceinline__ bool apply1(F1* x, int) const {
@@ -35,7 +35,7 @@ template <int M> struct SpecMulOp {
     const F2* b2; const F1* b1;
     template <int R> __device__ __forceinline__ bool apply2(F2* x, int g) const {
 #pragma unroll
-        for (int k = 0; k < R; ++k) x[k] = cmul(x[k], b2[k * ((1 << M) / R) + g]);
+        for (int k = 0; k < R; ++k) x[k] = lkmulc(x[k], b2[k * ((1 << M) / R) + g]);
         return false;
     }
     template <int R> __device__ __forceinline__ bool apply1(F1* x, int g) const {
@@ -45,12 +45,13 @@ template <int M> struct SpecMulOp {
     }
 };
 
-// Stores the spectrum in fused-pass order and stops (no inverse).
+// Stores the spectrum (canonical, as every multiplier constant is) in fused-pass order and
+// stops (no inverse).
 template <int M> struct SpecStoreOp {
     F2* b2; F1* b1;
     template <int R> __device__ __forceinline__ bool apply2(F2* x, int g) const {
 #pragma unroll
-        for (int k = 0; k < R; ++k) b2[k * ((1 << M) / R) + g] = x[k];
+        for (int k = 0; k < R; ++k) b2[k * ((1 << M) / R) + g] = lccanon(x[k]);
         return true;
     }
     template <int R> __device__ __forceinline__ bool apply1(F1* x, int g) const {
@@ -65,18 +66,22 @@ template <int M> struct SpecStoreOp {
 // index (h - rev(p)) mod h; in place, one thread per pair {p, q} (q = 3 * 2^a - 1 - p for p in
 // octave [2^a, 2^(a+1)), q = p for p < 2).
 template <int MH, int NT>
-__device__ __forceinline__ void half_pointwise(F2* s2, F1* s1, const F2* __restrict__ ab2, const F1* __restrict__ ab1) {
+__device__ __noinline__ void half_pointwise(F2* s2, F1* s1, const F2* __restrict__ ab2, const F1* __restrict__ ab1) {
     constexpr int H = 1 << MH;
+#pragma unroll 1
     for (int tau = threadIdx.x; tau < H / 2 + 1; tau += NT) {
         const int p = tau < 2 ? tau : tau - 1 + (1 << (31 - __clz(tau - 1)));
         const int q = p == 0 ? 0 : (3 << (31 - __clz(p))) - 1 - p;
         {
+            // e = z_p + conj z_q, d = z_p - conj z_q on reduced values, then e A + d B.
             const F2 zp = s2[swz(p)], zq = s2[swz(q)];
-            const F2 e = cadd(zp, cconj(zq)), d = csub(zp, cconj(zq));
-            const F2 op = cadd(cmul(e, ab2[p]), cmul(d, ab2[H + p]));
+            const F2 e = lcfold(f2(zp.re + zq.re, zp.im + lsub<2>(0, zq.im)));
+            const F2 d = lcfold(f2(lsub<2>(zp.re, zq.re), zp.im + zq.im));
+            const F2 op = lcfold(lcadd(lkmulc(e, ab2[p]), lkmulc(d, ab2[H + p])));
             if (q != p) {
-                const F2 e2 = cadd(zq, cconj(zp)), d2 = csub(zq, cconj(zp));
-                s2[swz(q)] = cadd(cmul(e2, ab2[q]), cmul(d2, ab2[H + q]));
+                const F2 e2 = lcfold(f2(zq.re + zp.re, zq.im + lsub<2>(0, zp.im)));
+                const F2 d2 = lcfold(f2(lsub<2>(zq.re, zp.re), zq.im + zp.im));
+                s2[swz(q)] = lcfold(lcadd(lkmulc(e2, ab2[q]), lkmulc(d2, ab2[H + q])));
             }
             s2[swz(p)] = op;
         }
@@ -100,10 +105,10 @@ template <int M> constexpr int smem_bytes() { return 24 << M; }
 // REDC from T (in tl, 2n limbs) into x (n limbs), wraparound path. Returns false on a carry
 // out that must vanish.
 template <int M, int NT>
-__device__ __forceinline__ bool redc_wrap(F2* s2, F1* s1, const uint32_t* tl, uint32_t* x, const F2* cc2, const F1* cc1,
-                                          const F2* tab2, const F1* tab1, uint64_t* sc) {
+__device__ __noinline__ bool redc_wrap(F2* s2, F1* s1, const uint32_t* tl, uint32_t* x, const F2* cc2, const F1* cc1,
+                                          const F2K* tab2, const F1* tab1, uint64_t* sc) {
     constexpr int N = 1 << M;
-    const F2* ht2 = tab2 + lt_half_off(M);
+    const F2K* ht2 = tab2 + lt_half_off(M);
     const F1* ht1 = tab1 + lt_half_off(M);
     fwd_limbs<M, NT>(tl, N, s2, s1, tab2, tab1);
     fused_mid<M, NT, true>(tl, N, s2, s1, tab2, tab1, SpecMulOp<M>{cc2, cc1});
@@ -176,7 +181,7 @@ __global__ void __launch_bounds__(NT) mul_kernel(SlotArgs a, uint32_t out, uint3
 // transform of N (cpu.rs:239-284; computed on the host by the reference's GPU backend).
 // inv8h = (8 h)^-1 in each field.
 template <int M, int NT>
-__global__ void __launch_bounds__(NT) setup_kernel(const uint32_t* nl, const uint32_t* npl, F2* c2, F1* c1, const F2* tab2,
+__global__ void __launch_bounds__(NT) setup_kernel(const uint32_t* nl, const uint32_t* npl, F2* c2, F1* c1, const F2K* tab2,
                                                    const F1* tab1, F2 inv8h2, F1 inv8h1, uint32_t first) {
     constexpr int N = 1 << M, H = N / 2;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -200,17 +205,17 @@ __global__ void __launch_bounds__(NT) setup_kernel(const uint32_t* nl, const uin
         s1[swz(j)] = z1;
     }
     __syncthreads();
-    const F2* ht2 = tab2 + lt_half_off(M);
+    const F2K* ht2 = tab2 + lt_half_off(M);
     const F1* ht1 = tab1 + lt_half_off(M);
     dif_unweighted<M - 1, NT>(s2, s1, ht2, ht1);
-    const F2* u2 = tab2 + lt_unpack_off(M);
+    const F2K* u2 = tab2 + lt_unpack_off(M);
     const F1* u1 = tab1 + lt_unpack_off(M);
     // half_nhat (cpu.rs:239-249) into elements h..2h.
     for (int p = threadIdx.x; p < H; p += NT) {
         const int q = p < 2 ? p : (3 << (31 - __clz(p))) - 1 - p;
         {
-            const F2 zk = s2[swz(p)], zj = cconj(s2[swz(q)]);
-            const F2 e = cadd(zk, zj), wo = cmul(mul_mi(csub(zk, zj)), u2[p]);
+            const F2 zk = lccanon(s2[swz(p)]), zj = cconj(lccanon(s2[swz(q)]));
+            const F2 e = cadd(zk, zj), wo = cmul(mul_mi(csub(zk, zj)), f2(u2[p].re, u2[p].im));
             const F2 xx = cadd(e, wo), yy = csub(e, wo);
             s2[swz(H + p)] = p == 0 ? cadd(cmul(xx, inv8h2), mul_i(cmul(yy, inv8h2))) : cmul(xx, inv8h2);
         }
@@ -228,10 +233,10 @@ __global__ void __launch_bounds__(NT) setup_kernel(const uint32_t* nl, const uin
         {
             const F2 sp = s2[swz(H + p)], sq = s2[swz(H + q)];
             const F2 nx = p == 0 ? f2(sp.re, 0) : sp, ny = p == 0 ? f2(sp.im, 0) : cconj(sq);
-            const F2 iu = u2[H + p], iiu = mul_i(iu);
+            const F2 iu = f2(u2[H + p].re, u2[H + p].im), iiu = mul_i(iu);
             const F2 X = cmul(nx, f2(add2(1, iiu.re), iiu.im)), Y = cmul(ny, f2(sub2(1, iiu.re), sub2(0, iiu.im)));
             o2[N + p] = cadd(X, Y);
-            o2[N + H + p] = cmul(mul_mi(csub(X, Y)), u2[p]);
+            o2[N + H + p] = cmul(mul_mi(csub(X, Y)), f2(u2[p].re, u2[p].im));
         }
         {
             const F1 sp = s1[swz(H + p)], sq = s1[swz(H + q)];

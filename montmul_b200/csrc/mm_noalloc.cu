@@ -34,7 +34,7 @@ static_assert(noalloc_bytes(kMaxSharedLogN) <= kNoAllocScratchBytes, "scratch to
 
 template <int M, int NT>
 __global__ void __launch_bounds__(NT) mul_noalloc_kernel(const uint32_t* a, const uint32_t* b, uint32_t* out,
-                                                          const F2* cc2, const F1* cc1, const F2* tab2,
+                                                          const F2* cc2, const F1* cc1, const F2K* tab2,
                                                           const F1* tab1, unsigned char* scratch, uint32_t* err) {
     constexpr int N = 1 << M;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -55,7 +55,7 @@ __global__ void __launch_bounds__(NT) mul_noalloc_kernel(const uint32_t* a, cons
     if (threadIdx.x == 0 && err) *err = ok ? 0u : 1u;
 }
 
-typedef void (*NoAllocFn)(const uint32_t*, const uint32_t*, uint32_t*, const F2*, const F1*, const F2*, const F1*,
+typedef void (*NoAllocFn)(const uint32_t*, const uint32_t*, uint32_t*, const F2*, const F1*, const F2K*, const F1*,
                           unsigned char*, uint32_t*);
 
 template <int M> NoAllocFn noalloc_fn() { return mul_noalloc_kernel<M, threads_for(M)>; }
@@ -115,14 +115,15 @@ static int noalloc_setup(int device, unsigned char** scratch, std::string& msg) 
 
 // Defined in mm_backend.cu: the batch fields this entry point reads, and the error message slot.
 extern "C++" int mm_batch_view(const mm_b200_batch* b, int* device, int* m, const mm::F2** c2, const mm::F1** c1,
-                               const mm::F2** tab2, const mm::F1** tab1, size_t* slots);
+                               const mm::F2K** tab2, const mm::F1** tab1, size_t* slots);
 extern "C++" int mm_set_error(int code, const std::string& msg);
 
 extern "C" int mm_b200_mul_noalloc(const mm_b200_batch* b, size_t slot, const uint32_t* d_a, const uint32_t* d_b,
                                    uint32_t* d_out, uint32_t* d_err, void* stream) {
     using namespace mm;
     int device = 0, m = 0;
-    const F2 *c2 = nullptr, *tab2 = nullptr;
+    const F2* c2 = nullptr;
+    const F2K* tab2 = nullptr;
     const F1 *c1 = nullptr, *tab1 = nullptr;
     size_t slots = 0;
     if (!b || !d_a || !d_b || !d_out) return mm_set_error(MM_ERR_ARG, "mul_noalloc: null argument");

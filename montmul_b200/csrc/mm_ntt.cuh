@@ -78,6 +78,57 @@ template <typename T> __device__ __forceinline__ void bf_dit8(T* x) {
     x[2] = cadd(a2, v2); x[6] = csub(a2, v2);
     x[3] = cadd(a3, v3); x[7] = csub(a3, v3);
 }
+// ---- lazy GF(M61^2) butterflies (inputs reduced, below 2^61 + 2^34) ----
+// DIF: outputs below 8 * 2^61, not reduced (the pass folds them or feeds them to a twiddle
+// product after a fold). DIT: outputs reduced. Offsets K p and fold points follow the interval
+// model of these exact operation sequences.
+__device__ __forceinline__ void ldif2(F2* x) { F2 u = x[0]; x[0] = lcadd(u, x[1]); x[1] = lcsub<2>(u, x[1]); }
+__device__ __forceinline__ void ldit2(F2* x) { F2 u = x[0]; x[0] = lcfold(lcadd(u, x[1])); x[1] = lcfold(lcsub<2>(u, x[1])); }
+__device__ __forceinline__ void ldif4(F2* x) {
+    const F2 a0 = lcadd(x[0], x[2]), b0 = lcsub<2>(x[0], x[2]);
+    const F2 a1 = lcadd(x[1], x[3]), b1 = lcsub_i<2>(x[1], x[3]);
+    x[0] = lcadd(a0, a1); x[1] = lcsub<3>(a0, a1);
+    x[2] = lcadd(b0, b1); x[3] = lcsub<4>(b0, b1);
+}
+__device__ __forceinline__ void ldit4(F2* x) {
+    const F2 c0 = lcadd(x[0], x[1]), c1 = lcsub<2>(x[0], x[1]);
+    const F2 c2 = lcadd(x[2], x[3]), c3 = lcsub<2>(x[2], x[3]);
+    x[0] = lcfold(lcadd(c0, c2)); x[2] = lcfold(lcsub<3>(c0, c2));
+    x[1] = lcfold(lcadd_mi<4>(c1, c3)); x[3] = lcfold(lcsub_mi<4>(c1, c3));
+}
+__device__ __forceinline__ void ldif8(F2* x) {
+    const F2 a0 = lcfold(lcadd(x[0], x[4])), b0 = lcfold(lcsub<2>(x[0], x[4]));
+    const F2 a1 = lcfold(lcadd(x[1], x[5])), b1 = lw8<4>(lcsub<2>(x[1], x[5]));
+    const F2 a2 = lcfold(lcadd(x[2], x[6])), b2 = lcfold(lcsub_i<2>(x[2], x[6]));
+    const F2 a3 = lcfold(lcadd(x[3], x[7])), b3 = lw8<4>(lcsub_i<2>(x[3], x[7]));
+    const F2 c0 = lcadd(a0, a2), c2 = lcsub<2>(a0, a2);
+    const F2 c1 = lcadd(a1, a3), c3 = lcsub_i<2>(a1, a3);
+    const F2 d0 = lcadd(b0, b2), d2 = lcsub<2>(b0, b2);
+    const F2 d1 = lcadd(b1, b3), d3 = lcsub_i<2>(b1, b3);
+    x[0] = lcadd(c0, c1); x[1] = lcsub<3>(c0, c1);
+    x[2] = lcadd(c2, c3); x[3] = lcsub<4>(c2, c3);
+    x[4] = lcadd(d0, d1); x[5] = lcsub<3>(d0, d1);
+    x[6] = lcadd(d2, d3); x[7] = lcsub<4>(d2, d3);
+}
+__device__ __forceinline__ void ldit8(F2* x) {
+    const F2 c0 = lcfold(lcadd(x[0], x[1])), c1 = lcfold(lcsub<2>(x[0], x[1]));
+    const F2 c2 = lcfold(lcadd(x[2], x[3])), c3 = lcfold(lcsub<2>(x[2], x[3]));
+    const F2 c4 = lcfold(lcadd(x[4], x[5])), c5 = lcfold(lcsub<2>(x[4], x[5]));
+    const F2 c6 = lcfold(lcadd(x[6], x[7])), c7 = lcfold(lcsub<2>(x[6], x[7]));
+    const F2 a0 = lcadd(c0, c2), a2 = lcsub<2>(c0, c2);
+    const F2 a1 = lcadd_mi<2>(c1, c3), a3 = lcsub_mi<2>(c1, c3);
+    const F2 b0 = lcadd(c4, c6), b2 = lcsub<2>(c4, c6);
+    const F2 b1 = lcadd_mi<2>(c5, c7), b3 = lcsub_mi<2>(c5, c7);
+    const F2 v1 = lv8<4>(b1), v3 = lv8<4>(lmi<4>(b3));
+    x[0] = lcfold(lcadd(a0, b0)); x[4] = lcfold(lcsub<3>(a0, b0));
+    x[1] = lcfold(lcadd(a1, v1)); x[5] = lcfold(lcsub<2>(a1, v1));
+    x[2] = lcfold(f2(a2.re + b2.im, lsub<4>(a2.im, b2.re)));
+    x[6] = lcfold(f2(lsub<4>(a2.re, b2.im), a2.im + b2.re));
+    x[3] = lcfold(lcadd(a3, v3)); x[7] = lcfold(lcsub<2>(a3, v3));
+}
+template <int R> __device__ __forceinline__ void ldif(F2* x) { if (R == 2) ldif2(x); else if (R == 4) ldif4(x); else ldif8(x); }
+template <int R> __device__ __forceinline__ void ldit(F2* x) { if (R == 2) ldit2(x); else if (R == 4) ldit4(x); else ldit8(x); }
+
 template <> __device__ __forceinline__ void bf_dif<4, F1>(F1* x) { bf_dif4(x); }
 template <> __device__ __forceinline__ void bf_dif<4, F2>(F2* x) { bf_dif4(x); }
 template <> __device__ __forceinline__ void bf_dit<4, F1>(F1* x) { bf_dit4(x); }
@@ -87,59 +138,66 @@ template <> __device__ __forceinline__ void bf_dif<8, F2>(F2* x) { bf_dif8(x); }
 template <> __device__ __forceinline__ void bf_dit<8, F1>(F1* x) { bf_dit8(x); }
 template <> __device__ __forceinline__ void bf_dit<8, F2>(F2* x) { bf_dit8(x); }
 
-// ---- one unweighted pass over the shared vector ----
-// M = log2 of the transform length, I = pass index (DIF order), TAB = pointer to this
-// transform's table (F2 and F1 arrays with the same indices). No twiddles when q = 1.
-template <int M, int I, bool FWD, int NT, bool WEIGHTED>
-__device__ __forceinline__ void smem_pass(F2* s2, F1* s1, const F2* tab2, const F1* tab1) {
-    constexpr int R = sched_radix(M, I), Q = sched_q(M, I);
-    constexpr int G = (1 << M) / R;
-    constexpr int toff = FWD ? tab_fwd_off(M, I, WEIGHTED) : tab_inv_off(M, I, WEIGHTED);
+// ---- one pass over the shared vector ----
+// A radix-R pass with span q = 2^lq over G = n/R groups, twiddles `t2`/`t1` laid out
+// [k-1][j] (TW) or none (span 1). One non-inlined function per (R, direction, TW) serves every
+// pass of every transform, which keeps the step loop's code within the instruction cache.
+template <int R, bool FWD, int NT, bool TW>
+__device__ __noinline__ void pass_rt(F2* s2, F1* s1, const F2K* __restrict__ t2, const F1* __restrict__ t1, int lq, int G) {
+    const int q = 1 << lq;
+#pragma unroll 1
     for (int g = threadIdx.x; g < G; g += NT) {
-        const int j = g & (Q - 1);
-        const int b = (g / Q) * (R * Q) + j;
+        const int j = g & (q - 1);
+        const int b = ((g >> lq) << (lq + ilog2c(R))) + j;
         {
             F2 x[R];
 #pragma unroll
-            for (int k = 0; k < R; ++k) x[k] = s2[swz(b + k * Q)];
+            for (int k = 0; k < R; ++k) x[k] = s2[swz(b + k * q)];
             if (FWD) {
-                bf_dif<R, F2>(x);
-                if (Q > 1) {
+                ldif<R>(x);
+                x[0] = lcfold(x[0]);
 #pragma unroll
-                    for (int k = 1; k < R; ++k) x[k] = cmul(x[k], tab2[toff + (k - 1) * Q + j]);
-                }
+                for (int k = 1; k < R; ++k) x[k] = TW ? lkmul(lcfold(x[k]), t2[(k - 1) * q + j]) : lcfold(x[k]);
             } else {
-                if (Q > 1) {
+                if (TW) {
 #pragma unroll
-                    for (int k = 1; k < R; ++k) x[k] = cmul(x[k], tab2[toff + (k - 1) * Q + j]);
+                    for (int k = 1; k < R; ++k) x[k] = lkmul(x[k], t2[(k - 1) * q + j]);
                 }
-                bf_dit<R, F2>(x);
+                ldit<R>(x);
             }
 #pragma unroll
-            for (int k = 0; k < R; ++k) s2[swz(b + k * Q)] = x[k];
+            for (int k = 0; k < R; ++k) s2[swz(b + k * q)] = x[k];
         }
         {
             F1 x[R];
 #pragma unroll
-            for (int k = 0; k < R; ++k) x[k] = s1[swz(b + k * Q)];
+            for (int k = 0; k < R; ++k) x[k] = s1[swz(b + k * q)];
             if (FWD) {
                 bf_dif<R, F1>(x);
-                if (Q > 1) {
+                if (TW) {
 #pragma unroll
-                    for (int k = 1; k < R; ++k) x[k] = cmul(x[k], tab1[toff + (k - 1) * Q + j]);
+                    for (int k = 1; k < R; ++k) x[k] = cmul(x[k], t1[(k - 1) * q + j]);
                 }
             } else {
-                if (Q > 1) {
+                if (TW) {
 #pragma unroll
-                    for (int k = 1; k < R; ++k) x[k] = cmul(x[k], tab1[toff + (k - 1) * Q + j]);
+                    for (int k = 1; k < R; ++k) x[k] = cmul(x[k], t1[(k - 1) * q + j]);
                 }
                 bf_dit<R, F1>(x);
             }
 #pragma unroll
-            for (int k = 0; k < R; ++k) s1[swz(b + k * Q)] = x[k];
+            for (int k = 0; k < R; ++k) s1[swz(b + k * q)] = x[k];
         }
     }
     __syncthreads();
+}
+
+// Pass I (DIF order) of the length-2^M transform; its table follows mm_common.h's layout.
+template <int M, int I, bool FWD, int NT, bool WEIGHTED>
+__device__ __forceinline__ void smem_pass(F2* s2, F1* s1, const F2K* tab2, const F1* tab1) {
+    constexpr int R = sched_radix(M, I), Q = sched_q(M, I);
+    constexpr int toff = FWD ? tab_fwd_off(M, I, WEIGHTED) : tab_inv_off(M, I, WEIGHTED);
+    pass_rt<R, FWD, NT, (Q > 1)>(s2, s1, tab2 + toff, tab1 + toff, ilog2c(Q), (1 << M) / R);
 }
 
 // ---- the weighted first DIF pass, straight from real limbs in global memory ----
@@ -152,14 +210,14 @@ template <> __device__ __forceinline__ F1 real_times<F1>(uint32_t v, F1 c) {
     s = min(s, s - P1);
     return cmul_r(s, c);
 }
-template <> __device__ __forceinline__ F2 real_times<F2>(uint32_t v, F2 c) { return cmul_r((uint64_t)v, c); }
 
 template <int M, int NT>
-__device__ __forceinline__ void dif_first_from_limbs(const uint32_t* __restrict__ lim, int cnt, F2* s2, F1* s1,
-                                                     const F2* tab2, const F1* tab1) {
+__device__ __noinline__ void dif_first_from_limbs(const uint32_t* __restrict__ lim, int cnt, F2* s2, F1* s1,
+                                                     const F2K* tab2, const F1* tab1) {
     constexpr int R = sched_radix(M, 0), Q = sched_q(M, 0);
     static_assert(Q > 1, "single-pass transforms use the fused pass");
     constexpr int toff = tab_fwd_off(M, 0, true), coff = tab_in_const_off(M, true);
+#pragma unroll 1
     for (int j = threadIdx.x; j < Q; j += NT) {
         uint32_t v[R];
 #pragma unroll
@@ -167,10 +225,10 @@ __device__ __forceinline__ void dif_first_from_limbs(const uint32_t* __restrict_
         {
             F2 x[R];
 #pragma unroll
-            for (int k = 0; k < R; ++k) x[k] = real_times<F2>(v[k], tab2[coff + k]);
-            bf_dif<R, F2>(x);
+            for (int k = 0; k < R; ++k) x[k] = lreal_times(v[k], tab2[coff + k]);
+            ldif<R>(x);
 #pragma unroll
-            for (int k = 0; k < R; ++k) s2[swz(j + k * Q)] = cmul(x[k], tab2[toff + k * Q + j]);
+            for (int k = 0; k < R; ++k) s2[swz(j + k * Q)] = lkmul(lcfold(x[k]), tab2[toff + k * Q + j]);
         }
         {
             F1 x[R];
@@ -187,20 +245,21 @@ __device__ __forceinline__ void dif_first_from_limbs(const uint32_t* __restrict_
 // ---- the weighted last DIT pass: unweights by zeta^-(j + k q) / n into natural order ----
 // REAL_ONLY: only the real parts are needed (the low half of the product, coefficients < n).
 template <int M, int NT, bool REAL_ONLY>
-__device__ __forceinline__ void dit_last_weighted(F2* s2, F1* s1, const F2* tab2, const F1* tab1) {
+__device__ __noinline__ void dit_last_weighted(F2* s2, F1* s1, const F2K* tab2, const F1* tab1) {
     constexpr int R = sched_radix(M, 0), Q = sched_q(M, 0);
     static_assert(Q > 1, "single-pass transforms use the fused pass");
     constexpr int toff = tab_inv_off(M, 0, true), coff = tab_out_const_off(M, true);
+#pragma unroll 1
     for (int j = threadIdx.x; j < Q; j += NT) {
         {
             F2 x[R];
 #pragma unroll
-            for (int k = 0; k < R; ++k) x[k] = cmul(s2[swz(j + k * Q)], tab2[toff + k * Q + j]);
-            bf_dit<R, F2>(x);
+            for (int k = 0; k < R; ++k) x[k] = lkmul(s2[swz(j + k * Q)], tab2[toff + k * Q + j]);
+            ldit<R>(x);
 #pragma unroll
             for (int k = 0; k < R; ++k) {
-                if (REAL_ONLY) s2[swz(j + k * Q)].re = cmul_re(x[k], tab2[coff + k]);
-                else s2[swz(j + k * Q)] = cmul(x[k], tab2[coff + k]);
+                if (REAL_ONLY) s2[swz(j + k * Q)].re = lkmul_re(x[k], tab2[coff + k]);
+                else s2[swz(j + k * Q)] = lkmul(x[k], tab2[coff + k]);
             }
         }
         {
@@ -222,31 +281,34 @@ __device__ __forceinline__ void dit_last_weighted(F2* s2, F1* s1, const F2* tab2
 // OP::apply2/apply1(x, g) transforms the R spectrum values of group g (positions R g + k).
 // With a single pass (M <= 3) the same pass is also the weighted first/last pass.
 template <int M, int NT, bool REAL_ONLY, class OP>
-__device__ __forceinline__ void fused_mid(const uint32_t* __restrict__ lim, int cnt, F2* s2, F1* s1,
-                                          const F2* tab2, const F1* tab1, const OP& op) {
+__device__ __noinline__ void fused_mid(const uint32_t* __restrict__ lim, int cnt, F2* s2, F1* s1,
+                                          const F2K* tab2, const F1* tab1, const OP& op) {
     constexpr int P = sched_passes(M);
     constexpr int R = sched_radix(M, P - 1);
     constexpr int G = (1 << M) / R;
     constexpr bool single = (P == 1);
     constexpr int cin = tab_in_const_off(M, true), cout = tab_out_const_off(M, true);
+#pragma unroll 1
     for (int g = threadIdx.x; g < G; g += NT) {
         {
             F2 x[R];
             if (single) {
 #pragma unroll
-                for (int k = 0; k < R; ++k) x[k] = real_times<F2>(k < cnt ? lim[k] : 0u, tab2[cin + k]);
+                for (int k = 0; k < R; ++k) x[k] = lreal_times(k < cnt ? lim[k] : 0u, tab2[cin + k]);
             } else {
 #pragma unroll
                 for (int k = 0; k < R; ++k) x[k] = s2[swz(R * g + k)];
             }
-            bf_dif<R, F2>(x);
+            ldif<R>(x);
+#pragma unroll
+            for (int k = 0; k < R; ++k) x[k] = lcfold(x[k]);
             if (!op.template apply2<R>(x, g)) {
-                bf_dit<R, F2>(x);
+                ldit<R>(x);
 #pragma unroll
                 for (int k = 0; k < R; ++k) {
                     if (single) {
-                        if (REAL_ONLY) s2[k].re = cmul_re(x[k], tab2[cout + k]);
-                        else s2[k] = cmul(x[k], tab2[cout + k]);
+                        if (REAL_ONLY) s2[k].re = lkmul_re(x[k], tab2[cout + k]);
+                        else s2[k] = lkmul(x[k], tab2[cout + k]);
                     } else {
                         s2[swz(R * g + k)] = x[k];
                     }
@@ -284,7 +346,7 @@ __device__ __forceinline__ void fused_mid(const uint32_t* __restrict__ lim, int 
 // Forward weighted transform of real limbs up to (not including) the last pass.
 template <int M, int NT>
 __device__ __forceinline__ void fwd_limbs(const uint32_t* __restrict__ lim, int cnt, F2* s2, F1* s1,
-                                          const F2* t2, const F1* t1) {
+                                          const F2K* t2, const F1* t1) {
     constexpr int P = sched_passes(M);
     if constexpr (P >= 2) {
         dif_first_from_limbs<M, NT>(lim, cnt, s2, s1, t2, t1);
@@ -297,7 +359,7 @@ __device__ __forceinline__ void fwd_limbs(const uint32_t* __restrict__ lim, int 
 
 // Inverse weighted transform from after the fused pass down to natural order.
 template <int M, int NT, bool REAL_ONLY>
-__device__ __forceinline__ void inv_to_natural(F2* s2, F1* s1, const F2* t2, const F1* t1) {
+__device__ __forceinline__ void inv_to_natural(F2* s2, F1* s1, const F2K* t2, const F1* t1) {
     constexpr int P = sched_passes(M);
     if constexpr (P >= 2) {
         if constexpr (P >= 5) smem_pass<M, 3, false, NT, true>(s2, s1, t2, t1);
@@ -309,7 +371,7 @@ __device__ __forceinline__ void inv_to_natural(F2* s2, F1* s1, const F2* t2, con
 
 // Unweighted transforms of the first 2^M elements (the wraparound path's length h), all in smem.
 template <int M, int NT>
-__device__ __forceinline__ void dif_unweighted(F2* s2, F1* s1, const F2* t2, const F1* t1) {
+__device__ __forceinline__ void dif_unweighted(F2* s2, F1* s1, const F2K* t2, const F1* t1) {
     constexpr int P = sched_passes(M);
     smem_pass<M, 0, true, NT, false>(s2, s1, t2, t1);
     if constexpr (P >= 2) smem_pass<M, 1, true, NT, false>(s2, s1, t2, t1);
@@ -319,7 +381,7 @@ __device__ __forceinline__ void dif_unweighted(F2* s2, F1* s1, const F2* t2, con
     static_assert(P <= 5, "schedule longer than the shared-memory lengths need");
 }
 template <int M, int NT>
-__device__ __forceinline__ void dit_unweighted(F2* s2, F1* s1, const F2* t2, const F1* t1) {
+__device__ __forceinline__ void dit_unweighted(F2* s2, F1* s1, const F2K* t2, const F1* t1) {
     constexpr int P = sched_passes(M);
     if constexpr (P >= 5) smem_pass<M, 4, false, NT, false>(s2, s1, t2, t1);
     if constexpr (P >= 4) smem_pass<M, 3, false, NT, false>(s2, s1, t2, t1);

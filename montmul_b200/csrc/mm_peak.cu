@@ -1,6 +1,7 @@
 // Integer roofline probe: the peak rate of "butterfly pairs" (one radix-2 butterfly, a GF(p^2)
 // product plus an add and a sub, in both GF(M31^2) and GF(M61^2)) with the kernels' own field
-// arithmetic, from independent register-resident chains on every SM. The fused step's
+// arithmetic (the lazy Karatsuba product and folded add/sub for M61, canonical M31), from
+// independent register-resident chains on every SM. The fused step's
 // algorithmic work is counted in the same unit, so achieved / peak is its integer-pipe
 // roofline fraction.
 #include <cuda_runtime.h>
@@ -23,14 +24,16 @@ __global__ void __launch_bounds__(256) bfly_peak_kernel(int iters, F2* out2, F1*
         u1[c] = f1(t * 31u + c, t + 5u * c + 1);
         v1[c] = f1(t * 131u + 3u * c, 7u + c);
     }
-    const F2 w2 = f2(0x123456789abcdefull & P2, 0x0fedcba987654321ull & P2);
+    const uint64_t wr = 0x123456789abcdefull & P2, wi = 0x0fedcba987654321ull & P2;
+    F2K w2;
+    w2.re = wr; w2.im = wi; w2.s = (wr + wi) % P2; w2.d = (wi + P2 - wr) % P2;
     const F1 w1 = f1(0x12345678u, 0x7654321u);
     for (int it = 0; it < iters; ++it) {
 #pragma unroll
         for (int c = 0; c < kPeakChains; ++c) {
-            const F2 m2 = cmul(v2[c], w2);
-            v2[c] = csub(u2[c], m2);
-            u2[c] = cadd(u2[c], m2);
+            const F2 m2 = lkmul(v2[c], w2);
+            v2[c] = lcfold(lcsub<2>(u2[c], m2));
+            u2[c] = lcfold(lcadd(u2[c], m2));
             const F1 m1 = cmul(v1[c], w1);
             v1[c] = csub(u1[c], m1);
             u1[c] = cadd(u1[c], m1);
@@ -40,7 +43,7 @@ __global__ void __launch_bounds__(256) bfly_peak_kernel(int iters, F2* out2, F1*
     F1 s1 = f1(0, 0);
 #pragma unroll
     for (int c = 0; c < kPeakChains; ++c) {
-        s2 = cadd(s2, cadd(u2[c], v2[c]));
+        s2 = cadd(s2, cadd(lccanon(u2[c]), lccanon(v2[c])));
         s1 = cadd(s1, cadd(u1[c], v1[c]));
     }
     out2[t] = s2;
