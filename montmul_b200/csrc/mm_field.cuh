@@ -178,8 +178,16 @@ __device__ __forceinline__ F2 lkmulc(F2 x, F2 w) {
 __device__ __forceinline__ uint64_t lkmul_re(F2 x, const F2K& w) {
     return lfold(lmul1(x.re, w.re) + lmul1(x.im, P2 - w.im));
 }
+// v c mod p for a 32-bit v and canonical c, reduced (below 2^61 + 2^32): two 32x32 products.
+// v c = p0 + p1 2^32 with p0 = v c_lo, p1 = v c_hi (c_hi < 2^29, so p1 + p0_hi < 2^62).
+__device__ __forceinline__ uint64_t lmul32(uint32_t v, uint64_t c) {
+    const uint64_t p0 = (uint64_t)v * (uint32_t)c;
+    const uint64_t m = (uint64_t)v * (uint32_t)(c >> 32) + (p0 >> 32);   // bits 32.. of v c
+    // v c = m 2^32 + p0_lo; mod p: (low 61 bits) + (v c >> 61) = ((m << 32 | p0_lo) & p) + (m >> 29)
+    return ((m << 32 | (uint32_t)p0) & P2) + (m >> 29);
+}
 // real 32-bit limb times a canonical constant, reduced.
-__device__ __forceinline__ F2 lreal_times(uint32_t v, const F2K& c) { return f2(lfold(lmul1(v, c.re)), lfold(lmul1(v, c.im))); }
+__device__ __forceinline__ F2 lreal_times(uint32_t v, const F2K& c) { return f2(lmul32(v, c.re), lmul32(v, c.im)); }
 // x^2 c for reduced x and c <= 4, reduced.
 __device__ __forceinline__ F2 lsqr_scale(F2 x, uint32_t c) {
     const uint64_t re = lfold(lmul1(x.re + x.im, lsub<2>(x.re, x.im)));
@@ -197,11 +205,16 @@ __device__ __forceinline__ void crt3(uint32_t c1, uint64_t c2, uint32_t& w0, uin
     c2 = lcanon(c2);
     uint32_t c2m = (uint32_t)(c2 & P1) + (uint32_t)(c2 >> 31);   // < 2^31 + 2^30
     c2m = min(c2m, c2m - P1);
-    uint32_t h = dbl1(sub1(c2m, c1));
-    unsigned __int128 v = (unsigned __int128)c2 + ((unsigned __int128)h << 61) - h;
-    w0 = (uint32_t)v;
-    w1 = (uint32_t)(v >> 32);
-    w2 = (uint32_t)(v >> 64);
+    const uint32_t h = dbl1(sub1(c2m, c1));
+    // C = c2 - h + h 2^61 = (c2 - h) + (h & 7) 2^61 + (h >> 3) 2^64, with the borrow of c2 - h
+    // and the carry of the low 64-bit sum folded into the top word.
+    const uint64_t t = c2 - h;
+    const uint32_t borrow = c2 < (uint64_t)h;
+    const uint64_t lo = t + ((uint64_t)(h & 7) << 61);
+    const uint32_t carry = lo < t;
+    w0 = (uint32_t)lo;
+    w1 = (uint32_t)(lo >> 32);
+    w2 = (h >> 3) + carry - borrow;
 }
 
 }  // namespace mm

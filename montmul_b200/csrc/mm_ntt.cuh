@@ -20,6 +20,9 @@ namespace mm {
 __device__ __forceinline__ int swz(int e) {
     return (e & ~15) | ((((e >> 3) ^ (e >> 6)) & 1) << 3) | ((e ^ (e >> 3)) & 7);
 }
+MM_HD constexpr int swz_c(int e) {
+    return (e & ~15) | ((((e >> 3) ^ (e >> 6)) & 1) << 3) | ((e ^ (e >> 3)) & 7);
+}
 
 // ---- in-register butterflies (positions k of one group) ----
 // u + (-i) v and u - (-i) v
@@ -139,20 +142,25 @@ template <> __device__ __forceinline__ void bf_dit<8, F1>(F1* x) { bf_dit8(x); }
 template <> __device__ __forceinline__ void bf_dit<8, F2>(F2* x) { bf_dit8(x); }
 
 // ---- one pass over the shared vector ----
-// A radix-R pass with span q = 2^lq over G = n/R groups, twiddles `t2`/`t1` laid out
-// [k-1][j] (TW) or none (span 1). One non-inlined function per (R, direction, TW) serves every
-// pass of every transform, which keeps the step loop's code within the instruction cache.
+// A radix-R pass with span q = 2^LQ over G = n/R groups, twiddles `t2`/`t1` laid out
+// [k-1][j] (TW) or none (span 1). One non-inlined function per (R, direction, TW) with a
+// runtime span serves every pass of every transform: the smaller code measured faster than one
+// instance per span, because the step loop's code then stays within the instruction cache.
 template <int R, bool FWD, int NT, bool TW>
-__device__ __noinline__ void pass_rt(F2* s2, F1* s1, const F2K* __restrict__ t2, const F1* __restrict__ t1, int lq, int G) {
-    const int q = 1 << lq;
+__device__ __noinline__ void pass_rt(F2* s2, F1* s1, const F2K* __restrict__ t2, const F1* __restrict__ t1, int LQ, int G) {
+    const int q = 1 << LQ;
+    int ko[R];   // swz(k q): the span is a runtime value, so the k offsets are formed once per pass
+#pragma unroll
+    for (int k = 0; k < R; ++k) ko[k] = swz(k * q);
 #pragma unroll 1
     for (int g = threadIdx.x; g < G; g += NT) {
         const int j = g & (q - 1);
-        const int b = ((g >> lq) << (lq + ilog2c(R))) + j;
+        // b + k q has disjoint bits, and swz is linear over XOR: swz(b + k q) = swz(b) ^ swz(k q).
+        const int sb = swz(((g >> LQ) << (LQ + ilog2c(R))) + j);
         {
             F2 x[R];
 #pragma unroll
-            for (int k = 0; k < R; ++k) x[k] = s2[swz(b + k * q)];
+            for (int k = 0; k < R; ++k) x[k] = s2[sb ^ ko[k]];
             if (FWD) {
                 ldif<R>(x);
                 x[0] = lcfold(x[0]);
@@ -166,12 +174,12 @@ __device__ __noinline__ void pass_rt(F2* s2, F1* s1, const F2K* __restrict__ t2,
                 ldit<R>(x);
             }
 #pragma unroll
-            for (int k = 0; k < R; ++k) s2[swz(b + k * q)] = x[k];
+            for (int k = 0; k < R; ++k) s2[sb ^ ko[k]] = x[k];
         }
         {
             F1 x[R];
 #pragma unroll
-            for (int k = 0; k < R; ++k) x[k] = s1[swz(b + k * q)];
+            for (int k = 0; k < R; ++k) x[k] = s1[sb ^ ko[k]];
             if (FWD) {
                 bf_dif<R, F1>(x);
                 if (TW) {
@@ -186,7 +194,7 @@ __device__ __noinline__ void pass_rt(F2* s2, F1* s1, const F2K* __restrict__ t2,
                 bf_dit<R, F1>(x);
             }
 #pragma unroll
-            for (int k = 0; k < R; ++k) s1[swz(b + k * q)] = x[k];
+            for (int k = 0; k < R; ++k) s1[sb ^ ko[k]] = x[k];
         }
     }
     __syncthreads();
