@@ -30,15 +30,19 @@ enum {
     MM_ERR_ARG = 1,          /* bad argument (index, size, unsupported length, ...) */
     MM_ERR_OOM = 2,          /* batch does not fit in device memory (message names the bytes) */
     MM_ERR_CARRY = 3,        /* a carry that must vanish did not (message names the slot) */
-    MM_ERR_CUDA = 4,         /* CUDA runtime error (message carries the runtime's text) */
+    MM_ERR_CUDA = 4,         /* CUDA runtime error (message carries the runtime's text), or a
+                                device copy that did not complete within its time limit */
     MM_ERR_UNSUPPORTED = 5   /* a configuration this build does not run */
 };
 
 typedef struct mm_b200_device mm_b200_device; /* `Gpu` (gpu/mod.rs:47-54): one CUDA device */
 typedef struct mm_b200_batch mm_b200_batch;   /* `GpuState` (gpu/mod.rs:237-258): one batch */
 
-/* `GpuOptions` (gpu/mod.rs:28-45). max_launch_steps bounds the steps of one kernel launch
- * (the reference bounds launches by time, max_launch_ms); 0 selects the default. */
+/* `GpuOptions` (gpu/mod.rs:28-45). Lengths L <= 16384 run with the whole vector in shared
+ * memory; longer ones (up to 2^24) keep it in device memory and stream 2,048-element tiles
+ * through shared memory ("global mode"). force_global selects global mode from L = 8192 on
+ * (the reference's force_global). max_launch_steps bounds the steps of one kernel launch (the
+ * reference bounds launches by time, max_launch_ms); 0 selects the default. */
 typedef struct {
     int device;
     int force_global;

@@ -108,8 +108,8 @@ class _Batch:
 class B200:
     """`Gpu`-equivalent backend on one B200 (wraparound path, k = L/2)."""
 
-    def __init__(self, device: int = 0, max_launch_steps: int = 0):
-        opts = Options(device, 0, 1, max_launch_steps)
+    def __init__(self, device: int = 0, max_launch_steps: int = 0, force_global: bool = False):
+        opts = Options(device, int(force_global), 1, max_launch_steps)
         ptr = _vp()
         _check(lib().mm_b200_open(C.byref(opts), C.byref(ptr)))
         self._dev = ptr

@@ -34,6 +34,27 @@ struct KernelSet {
     int smem;      // dynamic shared memory per block
 };
 
+// Global mode (kMaxSharedLogN < m <= kMaxGlobalLogN, or forced from m = 12): the same slot
+// state plus a per-slot work vector of n elements (F2 then F1 arrays, swizzled order).
+struct GArgs {
+    SlotArgs a;
+    F2* w2;   // slots x n
+    F1* w1;
+    int m;    // log2 n
+};
+typedef void (*GStepFn)(GArgs, uint32_t, uint32_t);
+typedef void (*GMulFn)(GArgs, uint32_t, uint32_t, uint32_t, F2*, F1*);
+typedef void (*GSetupFn)(GArgs, const uint32_t*, const uint32_t*, F2*, F1*, F2, F1, uint32_t);
+struct GlobalKernels {
+    GStepFn step;
+    GMulFn mul;
+    GSetupFn setup;
+    int threads;
+    int smem;
+};
+constexpr int kMinGlobalLogN = 12;   // smallest length the global kernels accept (one tile per half)
+GlobalKernels global_kernels();       // mm_global.cu
+
 // Threads per block for transform length 2^m: one radix-8 group per thread up to 256 threads.
 constexpr int threads_for(int m) { return m - 3 <= 5 ? 32 : (m - 3 >= 8 ? 256 : (1 << (m - 3))); }
 

@@ -71,6 +71,8 @@ struct mm_b200_device {
     int sms = 0;
     int max_smem = 0;
     int max_launch_steps = 512;
+    bool force_global = false;
+    bool global_configured = false;
     std::string name;
     std::mutex mu;
     std::map<int, DevTables> tables;
@@ -83,6 +85,10 @@ struct mm_b200_batch {
     size_t k = 0, n = 0, slots = 0;
     uint32_t base = 3;
     KernelSet ks{};
+    bool global = false;       // vector in HBM, tiles through shared memory (mm_global.cuh)
+    GlobalKernels gk{};
+    F2* d_w2 = nullptr;        // global mode: slots x n work elements
+    F1* d_w1 = nullptr;
     cudaStream_t stream = nullptr;
     uint32_t* d_x = nullptr;
     uint32_t* d_t = nullptr;
@@ -110,12 +116,14 @@ struct mm_b200_batch {
 
 namespace {
 
-int ensure_tables(mm_b200_device* dev, int m, const DevTables** out) {
+// Tables of length 2^(m+1) in the layout of the shared-memory kernels or of global mode.
+int ensure_tables(mm_b200_device* dev, int m, bool global, const DevTables** out) {
     std::lock_guard<std::mutex> lock(dev->mu);
-    auto it = dev->tables.find(m);
+    const int key = global ? 100 + m : m;
+    auto it = dev->tables.find(key);
     if (it == dev->tables.end()) {
-        std::vector<F2K> t2 = host::karatsuba_form(host::gen_length_tables<F2>(m));
-        std::vector<F1> t1 = host::gen_length_tables<F1>(m);
+        std::vector<F2K> t2 = host::karatsuba_form(global ? host::gen_global_length_tables<F2>(m) : host::gen_length_tables<F2>(m));
+        std::vector<F1> t1 = global ? host::gen_global_length_tables<F1>(m) : host::gen_length_tables<F1>(m);
         DevTables d;
         MM_CK(cudaMalloc(&d.t2, t2.size() * sizeof(F2K)));
         MM_CK(cudaMalloc(&d.t1, t1.size() * sizeof(F1)));
@@ -123,9 +131,18 @@ int ensure_tables(mm_b200_device* dev, int m, const DevTables** out) {
         MM_CK(cudaMemcpy(d.t1, t1.data(), t1.size() * sizeof(F1), cudaMemcpyHostToDevice));
         d.inv8h2 = host::inv8h<F2>(m);
         d.inv8h1 = host::inv8h<F1>(m);
-        it = dev->tables.emplace(m, d).first;
+        it = dev->tables.emplace(key, d).first;
     }
-    if (!dev->configured[m]) {
+    if (global && !dev->global_configured) {
+        const GlobalKernels gk = global_kernels();
+        MM_CK(cudaFuncSetAttribute((const void*)gk.step, cudaFuncAttributeMaxDynamicSharedMemorySize, gk.smem));
+        MM_CK(cudaFuncSetAttribute((const void*)gk.mul, cudaFuncAttributeMaxDynamicSharedMemorySize, gk.smem));
+        MM_CK(cudaFuncSetAttribute((const void*)gk.setup, cudaFuncAttributeMaxDynamicSharedMemorySize, gk.smem));
+        MM_CK(cudaFuncSetAttribute((const void*)gk.step, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                   cudaSharedmemCarveoutMaxShared));
+        dev->global_configured = true;
+    }
+    if (!global && !dev->configured[m]) {
         KernelSet ks;
         kernel_set(m, ks);
         MM_CK(cudaFuncSetAttribute((const void*)ks.step, cudaFuncAttributeMaxDynamicSharedMemorySize, ks.smem));
@@ -138,6 +155,8 @@ int ensure_tables(mm_b200_device* dev, int m, const DevTables** out) {
     *out = &it->second;
     return MM_OK;
 }
+
+GArgs global_args(const mm_b200_batch* b);
 
 SlotArgs slot_args(const mm_b200_batch* b) {
     SlotArgs a;
@@ -154,6 +173,15 @@ SlotArgs slot_args(const mm_b200_batch* b) {
     a.ew = (uint32_t)b->ew;
     a.base = b->base;
     return a;
+}
+
+GArgs global_args(const mm_b200_batch* b) {
+    GArgs g;
+    g.a = slot_args(b);
+    g.w2 = b->d_w2;
+    g.w1 = b->d_w1;
+    g.m = b->m;
+    return g;
 }
 
 int pull_x(mm_b200_batch* b) {
@@ -211,6 +239,9 @@ int check_err(mm_b200_batch* b, const char* what) {
         if (err[i]) {
             MM_CK(cudaMemsetAsync(b->d_err, 0, b->slots * 4, b->stream));
             MM_CK(cudaStreamSynchronize(b->stream));
+            if (err[i] == 2)
+                return fail(MM_ERR_CUDA, std::string(what) + ": a bulk copy of slot " + std::to_string(i) +
+                                             " did not complete within its time limit");
             return fail(MM_ERR_CARRY, std::string(what) + ": carry out of a product that must fit, slot " + std::to_string(i));
         }
     }
@@ -225,10 +256,12 @@ int launch_steps(mm_b200_batch* b, size_t bits) {
     int rc = push(b);
     if (rc) return rc;
     const SlotArgs a = slot_args(b);
+    const GArgs g = global_args(b);
     const size_t chunk = (size_t)std::max(1, b->dev->max_launch_steps);
     while (left > 0) {
         const uint32_t s = (uint32_t)std::min(left, chunk);
-        b->ks.step<<<(unsigned)b->slots, b->ks.threads, b->ks.smem, b->stream>>>(a, 0, s);
+        if (b->global) b->gk.step<<<(unsigned)b->slots, b->gk.threads, b->gk.smem, b->stream>>>(g, 0, s);
+        else b->ks.step<<<(unsigned)b->slots, b->ks.threads, b->ks.smem, b->stream>>>(a, 0, s);
         MM_CK(cudaGetLastError());
         ++b->launches;
         for (size_t i = 0; i < b->slots; ++i) b->pos[i] += std::min<uint32_t>(s, b->nbits[i] - b->pos[i]);
@@ -264,7 +297,6 @@ int mm_b200_open(const mm_b200_options* opts, mm_b200_device** out) {
     mm_b200_options o{0, 0, 1, 0};
     if (opts) o = *opts;
     if (!o.wraparound) return fail(MM_ERR_UNSUPPORTED, "this backend runs the wraparound path only (k = L/2)");
-    if (o.force_global) return fail(MM_ERR_UNSUPPORTED, "global mode is not built in this version");
     if (!host::check_fixed_roots()) return fail(MM_ERR_UNSUPPORTED, "field roots differ from the ones the kernels assume");
     int count = 0;
     MM_CK(cudaGetDeviceCount(&count));
@@ -278,6 +310,7 @@ int mm_b200_open(const mm_b200_options* opts, mm_b200_device** out) {
     d->max_smem = (int)prop.sharedMemPerBlockOptin;
     d->name = prop.name;
     if (o.max_launch_steps > 0) d->max_launch_steps = o.max_launch_steps;
+    d->force_global = o.force_global != 0;
     *out = d;
     return MM_OK;
 }
@@ -312,7 +345,7 @@ void mm_b200_coefficient_bound(uint64_t out[2]) {
 
 size_t mm_b200_supported_lengths(size_t* out, size_t cap) {
     size_t cnt = 0;
-    for (int m = kMinLogN; m <= kMaxSharedLogN; ++m) {
+    for (int m = kMinLogN; m <= kMaxGlobalLogN; ++m) {
         if (out && cnt < cap) out[cnt] = (size_t)2 << m;
         ++cnt;
     }
@@ -324,10 +357,12 @@ int mm_b200_full_k(const mm_b200_device*) { return 1; }
 size_t mm_b200_batch_bytes(size_t slots, size_t len, size_t exp_words) {
     const size_t n = len / 2;
     // x (4n), T (8n), constants F(N') and A|B (2n elements of 24 B), exponent words, nbits,
-    // pos and err, per slot; plus mul's spectrum scratch (24n) and this length's tables.
-    const size_t per_slot = 4 * n + 8 * n + 48 * n + 4 * exp_words + 12;
+    // pos and err, per slot; plus mul's spectrum scratch (24n) and this length's tables. Global
+    // mode (n > 8192) adds the per-slot work vector (24n).
     const int m = log2_exact(n);
-    const size_t tabs = m >= kMinLogN ? (size_t)lt_size(m) * (sizeof(F2K) + sizeof(F1)) : 0;
+    const bool global = m > kMaxSharedLogN;
+    const size_t per_slot = 4 * n + 8 * n + 48 * n + (global ? 24 * n : 0) + 4 * exp_words + 12;
+    const size_t tabs = m < kMinLogN ? 0 : (size_t)(global ? glt_size(m) : lt_size(m)) * (sizeof(F2K) + sizeof(F1));
     return slots * per_slot + 24 * n + tabs;
 }
 
@@ -338,17 +373,22 @@ int mm_b200_create(mm_b200_device* dev, size_t k, size_t len, uint32_t base, siz
     if (slots == 0) return fail(MM_ERR_ARG, "empty batch");
     const int m = log2_exact(len / 2);
     if (len < 8 || m < kMinLogN || ((size_t)2 << m) != len) return fail(MM_ERR_ARG, "transform length must be a power of two >= 8");
-    if (m > kMaxSharedLogN) return fail(MM_ERR_UNSUPPORTED, "transform length " + std::to_string(len) + " needs global mode, not built in this version");
+    if (m > kMaxGlobalLogN) return fail(MM_ERR_UNSUPPORTED, "transform length " + std::to_string(len) + " exceeds the largest supported (2^24)");
+    const bool global = m > kMaxSharedLogN || (dev->force_global && m >= kMinGlobalLogN);
     if (k != len / 2) return fail(MM_ERR_ARG, "wraparound needs k = L/2");
     if (base < 1 || base > 4) return fail(MM_ERR_ARG, "base must be in 1..4 (lazy range)");
     MM_CK(cudaSetDevice(dev->device));
-    const size_t need = mm_b200_batch_bytes(slots, len, 1) + 8 * slots * k + ((size_t)64 << 20);
+    // batch_bytes counts global mode's work vectors from n > 8192 on; forced global mode below
+    // that adds them here.
+    const size_t forced = global && m <= kMaxSharedLogN ? 24 * slots * k : 0;
+    const size_t need = mm_b200_batch_bytes(slots, len, 1) + 8 * slots * k + forced + ((size_t)64 << 20);
     const size_t freeb = mm_b200_free_memory(dev);
     if (need > freeb) return fail(MM_ERR_OOM, "batch needs " + std::to_string(need) + " bytes, " + std::to_string(freeb) + " free");
     const DevTables* tab = nullptr;
-    int rc = ensure_tables(dev, m, &tab);
+    int rc = ensure_tables(dev, m, global, &tab);
     if (rc) return rc;
-    std::unique_ptr<mm_b200_batch> b(new mm_b200_batch());
+    // On a failure below, everything allocated so far is released with the batch.
+    std::unique_ptr<mm_b200_batch, void (*)(mm_b200_batch*)> b(new mm_b200_batch(), mm_b200_destroy);
     b->dev = dev;
     b->m = m;
     b->k = k;
@@ -356,7 +396,9 @@ int mm_b200_create(mm_b200_device* dev, size_t k, size_t len, uint32_t base, siz
     b->slots = slots;
     b->base = base;
     b->tab = tab;
-    kernel_set(m, b->ks);
+    b->global = global;
+    if (global) b->gk = global_kernels();
+    else kernel_set(m, b->ks);
     MM_CK(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
     const size_t nn = b->n;
     MM_CK(cudaMalloc(&b->d_x, slots * k * 4));
@@ -371,6 +413,10 @@ int mm_b200_create(mm_b200_device* dev, size_t k, size_t len, uint32_t base, siz
     MM_CK(cudaMalloc(&b->d_err, slots * 4));
     MM_CK(cudaMalloc(&b->d_spec2, nn * sizeof(F2)));
     MM_CK(cudaMalloc(&b->d_spec1, nn * sizeof(F1)));
+    if (global) {
+        MM_CK(cudaMalloc(&b->d_w2, slots * nn * sizeof(F2)));
+        MM_CK(cudaMalloc(&b->d_w1, slots * nn * sizeof(F1)));
+    }
     MM_CK(cudaMemsetAsync(b->d_x, 0, slots * k * 4, b->stream));
     MM_CK(cudaMemsetAsync(b->d_exp, 0, slots * 4, b->stream));
     MM_CK(cudaMemsetAsync(b->d_nbits, 0, slots * 4, b->stream));
@@ -384,14 +430,20 @@ int mm_b200_create(mm_b200_device* dev, size_t k, size_t len, uint32_t base, siz
     MM_CK(cudaMemcpyAsync(d_np, nprime, slots * k * 4, cudaMemcpyHostToDevice, b->stream));
     for (size_t first = 0; first < slots; first += 65535) {
         const unsigned grid = (unsigned)std::min<size_t>(65535, slots - first);
-        b->ks.setup<<<grid, b->ks.threads, b->ks.smem, b->stream>>>(d_n, d_np, b->d_c2, b->d_c1, tab->t2, tab->t1, tab->inv8h2,
-                                                                   tab->inv8h1, (uint32_t)first);
+        if (global)
+            b->gk.setup<<<grid, b->gk.threads, b->gk.smem, b->stream>>>(global_args(b.get()), d_n, d_np, b->d_c2, b->d_c1,
+                                                                       tab->inv8h2, tab->inv8h1, (uint32_t)first);
+        else
+            b->ks.setup<<<grid, b->ks.threads, b->ks.smem, b->stream>>>(d_n, d_np, b->d_c2, b->d_c1, tab->t2, tab->t1,
+                                                                       tab->inv8h2, tab->inv8h1, (uint32_t)first);
         MM_CK(cudaGetLastError());
         ++b->launches;
     }
     MM_CK(cudaStreamSynchronize(b->stream));
     MM_CK(cudaFree(d_n));
     MM_CK(cudaFree(d_np));
+    rc = check_err(b.get(), "create");
+    if (rc) return rc;
     MM_CK(cudaMallocHost(&b->host_x, slots * k * 4));
     b->host_x_len = slots * k;
     std::memset(b->host_x, 0, slots * k * 4);
@@ -474,8 +526,12 @@ int mm_b200_mul(mm_b200_batch* b, size_t out, size_t a, size_t bb) {
     MM_CK(cudaSetDevice(b->dev->device));
     int rc = push(b);
     if (rc) return rc;
-    b->ks.mul<<<1, b->ks.threads, b->ks.smem, b->stream>>>(slot_args(b), (uint32_t)out, (uint32_t)a, (uint32_t)bb, b->d_spec2,
-                                                          b->d_spec1);
+    if (b->global)
+        b->gk.mul<<<1, b->gk.threads, b->gk.smem, b->stream>>>(global_args(b), (uint32_t)out, (uint32_t)a, (uint32_t)bb,
+                                                              b->d_spec2, b->d_spec1);
+    else
+        b->ks.mul<<<1, b->ks.threads, b->ks.smem, b->stream>>>(slot_args(b), (uint32_t)out, (uint32_t)a, (uint32_t)bb,
+                                                              b->d_spec2, b->d_spec1);
     MM_CK(cudaGetLastError());
     ++b->launches;
     MM_CK(cudaStreamSynchronize(b->stream));
@@ -524,6 +580,8 @@ void mm_b200_destroy(mm_b200_batch* b) {
     cudaFree(b->d_err);
     cudaFree(b->d_spec2);
     cudaFree(b->d_spec1);
+    cudaFree(b->d_w2);
+    cudaFree(b->d_w1);
     if (b->stream) cudaStreamDestroy(b->stream);
     if (b->host_x) cudaFreeHost(b->host_x);
     if (b->host_exp) cudaFreeHost(b->host_exp);

@@ -101,3 +101,47 @@ MM_HD constexpr int const_index(int m, int p) {
 }
 
 }  // namespace mm
+
+namespace mm {
+
+// ---- global mode: the vector in HBM, transformed through shared-memory tiles ----
+// Lengths n = 2^m > kMaxSharedLogN. DIF stages whose span reaches a tile (2^kTileLog elements)
+// run as passes over global memory; the remaining kTileLog stages are, on every tile, exactly a
+// complete length-2^kTileLog transform (the twiddles of a stage depend only on its span), so the
+// tiles reuse one unweighted length-2^kTileLog table. DIT mirrors this.
+constexpr int kTileLog = 11;                  // 2,048-element tiles (48 KiB of F2 + F1)
+constexpr int kMaxGlobalLogN = 23;            // L = 2^24, the reference's largest length
+
+// Global passes of a length-2^m transform: the schedule of its G = m - kTileLog global stages.
+MM_HD int gl_stages(int m) { return m - kTileLog; }
+MM_HD int gl_passes(int m) { return sched_passes(gl_stages(m)); }
+MM_HD int gl_radix(int m, int i) { return sched_radix(gl_stages(m), i); }
+MM_HD int gl_lq(int m, int i) {
+    int lq = m;
+    for (int p = 0; p <= i; ++p) lq -= ilog2c(gl_radix(m, p));
+    return lq;
+}
+MM_HD int gl_pass_size(int m, int i, bool weighted) {
+    const int R = gl_radix(m, i), q = 1 << gl_lq(m, i);
+    return weighted && i == 0 ? R * q : (R - 1) * q;
+}
+MM_HD int gl_fwd_off(int m, int i, bool weighted) {
+    int o = 0;
+    for (int p = 0; p < i; ++p) o += gl_pass_size(m, p, weighted);
+    return o;
+}
+MM_HD int gl_fwd_size(int m, bool weighted) { return gl_fwd_off(m, gl_passes(m), weighted); }
+MM_HD int gl_inv_off(int m, int i, bool weighted) { return gl_fwd_size(m, weighted) + gl_fwd_off(m, i, weighted); }
+MM_HD int gl_in_const_off(int m, bool weighted) { return 2 * gl_fwd_size(m, weighted); }
+MM_HD int gl_out_const_off(int m, bool weighted) { return gl_in_const_off(m, weighted) + (weighted ? gl_radix(m, 0) : 0); }
+MM_HD int gl_tab_size(int m, bool weighted) { return gl_out_const_off(m, weighted) + (weighted ? gl_radix(m, 0) : 0); }
+
+// Tables of global-mode length L = 2^(m+1): the weighted full transform's global passes, the
+// tile transform (unweighted, length 2^kTileLog), the half transform's global passes (or none
+// when the half length fits one tile), then the wraparound unpack roots over h positions.
+MM_HD int glt_tile_off(int m) { return gl_tab_size(m, true); }
+MM_HD int glt_half_off(int m) { return glt_tile_off(m) + tab_size(kTileLog, false); }
+MM_HD int glt_unpack_off(int m) { return glt_half_off(m) + (m - 1 > kTileLog ? gl_tab_size(m - 1, false) : 0); }
+MM_HD int glt_size(int m) { return glt_unpack_off(m) + 2 * (1 << (m - 1)); }
+
+}  // namespace mm

@@ -150,6 +150,66 @@ template <class E> inline std::vector<E> gen_length_tables(int m) {
     return t;
 }
 
+// The global passes of a length-2^m transform (weighted or not) into t[0 .. gl_tab_size).
+// Same roots as gen_transform; powers are formed by repeated multiplication.
+template <class E> inline void gen_global_transform(int m, bool weighted, E* t) {
+    E omega, zeta;
+    roots<E>(m, omega, zeta);
+    const uint64_t n = 1ull << m;
+    const E zi = Gf<E>::inv(zeta);
+    for (int i = 0; i < gl_passes(m); ++i) {
+        const int R = gl_radix(m, i), lr = ilog2c(R);
+        const uint64_t q = 1ull << gl_lq(m, i);
+        const E W = gpow(omega, n / (R * q)), V = Gf<E>::inv(W);
+        E* f = t + gl_fwd_off(m, i, weighted);
+        E* b = t + gl_inv_off(m, i, weighted);
+        const bool w0 = weighted && i == 0;
+        for (int k = w0 ? 0 : 1; k < R; ++k) {
+            const int row = w0 ? k : k - 1;
+            const uint64_t rk = (uint64_t)rev_bits(k, lr);
+            const E fs = gpow(W, rk), bs = gpow(V, rk);
+            E fw = one<E>(), bw = one<E>(), zf = one<E>(), zb = one<E>();
+            for (uint64_t j = 0; j < q; ++j) {
+                f[row * q + j] = w0 ? Gf<E>::mul(fw, zf) : fw;
+                b[row * q + j] = w0 ? Gf<E>::mul(bw, zb) : bw;
+                fw = Gf<E>::mul(fw, fs);
+                bw = Gf<E>::mul(bw, bs);
+                if (w0) { zf = Gf<E>::mul(zf, zeta); zb = Gf<E>::mul(zb, zi); }
+            }
+        }
+    }
+    if (weighted) {
+        const int R0 = gl_radix(m, 0);
+        const uint64_t q0 = 1ull << gl_lq(m, 0);
+        const E ninv = Gf<E>::inv(Gf<E>::from(n));
+        for (int k = 0; k < R0; ++k) {
+            t[gl_in_const_off(m, true) + k] = gpow(zeta, q0 * k);
+            t[gl_out_const_off(m, true) + k] = Gf<E>::mul(gpow(zi, q0 * k), ninv);
+        }
+    }
+}
+
+// All tables of global-mode length L = 2^(m+1) (layout glt_* of mm_common.h).
+template <class E> inline std::vector<E> gen_global_length_tables(int m) {
+    std::vector<E> t(glt_size(m), E{});
+    gen_global_transform<E>(m, true, t.data());
+    gen_transform<E>(kTileLog, false, t.data() + glt_tile_off(m));
+    if (m - 1 > kTileLog) gen_global_transform<E>(m - 1, false, t.data() + glt_half_off(m));
+    E omega, zeta;
+    roots<E>(m, omega, zeta);
+    const E wi = Gf<E>::inv(omega);
+    const int h = 1 << (m - 1);
+    std::vector<E> pw(h), pwi(h);   // omega^j and omega^-j, j < h
+    E a = one<E>(), b = one<E>();
+    for (int j = 0; j < h; ++j) { pw[j] = a; pwi[j] = b; a = Gf<E>::mul(a, omega); b = Gf<E>::mul(b, wi); }
+    for (int p = 0; p < h; ++p) {
+        const int r = rev_bits(p, m - 1);
+        t[glt_unpack_off(m) + p] = pw[r];
+        t[glt_unpack_off(m) + h + p] = pwi[r];
+    }
+    return t;
+}
+
 // M61 tables as the device's Karatsuba products read them: (re, im, re + im, im - re) mod p.
 inline std::vector<F2K> karatsuba_form(const std::vector<F2>& t) {
     std::vector<F2K> out(t.size());

@@ -64,36 +64,100 @@ template <int M> struct SpecStoreOp {
 // ---- the wraparound half-pointwise step (cpu.rs:221-237, 261-284) ----
 // out_p = (z_p + conj z_q) A_p + (z_p - conj z_q) B_p with q = partner(p), the position of
 // index (h - rev(p)) mod h; in place, one thread per pair {p, q} (q = 3 * 2^a - 1 - p for p in
-// octave [2^a, 2^(a+1)), q = p for p < 2).
+// octave [2^a, 2^(a+1)), q = p for p < 2). The vector (h elements at swz(p)) may be in shared
+// or global memory.
+__device__ __forceinline__ void half_pointwise_pair(F2* s2, F1* s1, int H, const F2* __restrict__ ab2,
+                                                    const F1* __restrict__ ab1, int tau) {
+    const int p = tau < 2 ? tau : tau - 1 + (1 << (31 - __clz(tau - 1)));
+    const int q = p == 0 ? 0 : (3 << (31 - __clz(p))) - 1 - p;
+    {
+        // e = z_p + conj z_q, d = z_p - conj z_q on reduced values, then e A + d B.
+        const F2 zp = s2[swz(p)], zq = s2[swz(q)];
+        const F2 e = lcfold(f2(zp.re + zq.re, zp.im + lsub<2>(0, zq.im)));
+        const F2 d = lcfold(f2(lsub<2>(zp.re, zq.re), zp.im + zq.im));
+        const F2 op = lcfold(lcadd(lkmulc(e, ab2[p]), lkmulc(d, ab2[H + p])));
+        if (q != p) {
+            const F2 e2 = lcfold(f2(zq.re + zp.re, zq.im + lsub<2>(0, zp.im)));
+            const F2 d2 = lcfold(f2(lsub<2>(zq.re, zp.re), zq.im + zp.im));
+            s2[swz(q)] = lcfold(lcadd(lkmulc(e2, ab2[q]), lkmulc(d2, ab2[H + q])));
+        }
+        s2[swz(p)] = op;
+    }
+    {
+        const F1 zp = s1[swz(p)], zq = s1[swz(q)];
+        const F1 e = cadd(zp, cconj(zq)), d = csub(zp, cconj(zq));
+        const F1 op = cadd(cmul(e, ab1[p]), cmul(d, ab1[H + p]));
+        if (q != p) {
+            const F1 e2 = cadd(zq, cconj(zp)), d2 = csub(zq, cconj(zp));
+            s1[swz(q)] = cadd(cmul(e2, ab1[q]), cmul(d2, ab1[H + q]));
+        }
+        s1[swz(p)] = op;
+    }
+}
+
 template <int MH, int NT>
 __device__ __noinline__ void half_pointwise(F2* s2, F1* s1, const F2* __restrict__ ab2, const F1* __restrict__ ab1) {
     constexpr int H = 1 << MH;
 #pragma unroll 1
-    for (int tau = threadIdx.x; tau < H / 2 + 1; tau += NT) {
-        const int p = tau < 2 ? tau : tau - 1 + (1 << (31 - __clz(tau - 1)));
-        const int q = p == 0 ? 0 : (3 << (31 - __clz(p))) - 1 - p;
+    for (int tau = threadIdx.x; tau < H / 2 + 1; tau += NT) half_pointwise_pair(s2, s1, H, ab2, ab1, tau);
+    __syncthreads();
+}
+
+// half_forward's packing (cpu.rs:286-295): z_j = v_2j + i v_2j+1 for j < h, at swz(j). Ends
+// with a barrier.
+__device__ __forceinline__ void pack_pairs(const uint32_t* __restrict__ v, F2* s2, F1* s1, int H, int nt) {
+    for (int j = threadIdx.x; j < H; j += nt) {
+        const uint32_t v0 = v[2 * j], v1 = v[2 * j + 1];
+        F2 z2; z2.re = v0; z2.im = v1;
+        const uint32_t r0 = (v0 & P1) + (v0 >> 31), r1 = (v1 & P1) + (v1 >> 31);
+        F1 z1; z1.re = min(r0, r0 - P1); z1.im = min(r1, r1 - P1);
+        s2[swz(j)] = z2;
+        s1[swz(j)] = z1;
+    }
+    __syncthreads();
+}
+
+// ---- wraparound factors of one modulus from the half transform of N (cpu.rs:239-284) ----
+// In: the unweighted length-h DIF of z_j = N_2j + i N_2j+1 in elements [0, h) (at swz). Writes
+// half_nhat into elements [h, 2h), then A (ab[p]) and B (ab[h + p]). u: unpack roots w^rev(p)
+// (p < h) and w^-rev(p) (h + p). inv8h = (8 h)^-1. Ends with a barrier.
+__device__ __forceinline__ void half_factors_block(F2* s2, F1* s1, int H, const F2K* u2, const F1* u1, F2* ab2, F1* ab1,
+                                                   F2 inv8h2, F1 inv8h1, int nt) {
+    // half_nhat (cpu.rs:239-249) into elements h..2h.
+    for (int p = threadIdx.x; p < H; p += nt) {
+        const int q = p < 2 ? p : (3 << (31 - __clz(p))) - 1 - p;
         {
-            // e = z_p + conj z_q, d = z_p - conj z_q on reduced values, then e A + d B.
-            const F2 zp = s2[swz(p)], zq = s2[swz(q)];
-            const F2 e = lcfold(f2(zp.re + zq.re, zp.im + lsub<2>(0, zq.im)));
-            const F2 d = lcfold(f2(lsub<2>(zp.re, zq.re), zp.im + zq.im));
-            const F2 op = lcfold(lcadd(lkmulc(e, ab2[p]), lkmulc(d, ab2[H + p])));
-            if (q != p) {
-                const F2 e2 = lcfold(f2(zq.re + zp.re, zq.im + lsub<2>(0, zp.im)));
-                const F2 d2 = lcfold(f2(lsub<2>(zq.re, zp.re), zq.im + zp.im));
-                s2[swz(q)] = lcfold(lcadd(lkmulc(e2, ab2[q]), lkmulc(d2, ab2[H + q])));
-            }
-            s2[swz(p)] = op;
+            const F2 zk = lccanon(s2[swz(p)]), zj = cconj(lccanon(s2[swz(q)]));
+            const F2 e = cadd(zk, zj), wo = cmul(mul_mi(csub(zk, zj)), f2(u2[p].re, u2[p].im));
+            const F2 xx = cadd(e, wo), yy = csub(e, wo);
+            s2[swz(H + p)] = p == 0 ? cadd(cmul(xx, inv8h2), mul_i(cmul(yy, inv8h2))) : cmul(xx, inv8h2);
         }
         {
-            const F1 zp = s1[swz(p)], zq = s1[swz(q)];
-            const F1 e = cadd(zp, cconj(zq)), d = csub(zp, cconj(zq));
-            const F1 op = cadd(cmul(e, ab1[p]), cmul(d, ab1[H + p]));
-            if (q != p) {
-                const F1 e2 = cadd(zq, cconj(zp)), d2 = csub(zq, cconj(zp));
-                s1[swz(q)] = cadd(cmul(e2, ab1[q]), cmul(d2, ab1[H + q]));
-            }
-            s1[swz(p)] = op;
+            const F1 zk = s1[swz(p)], zj = cconj(s1[swz(q)]);
+            const F1 e = cadd(zk, zj), wo = cmul(mul_mi(csub(zk, zj)), u1[p]);
+            const F1 xx = cadd(e, wo), yy = csub(e, wo);
+            s1[swz(H + p)] = p == 0 ? cadd(cmul(xx, inv8h1), mul_i(cmul(yy, inv8h1))) : cmul(xx, inv8h1);
+        }
+    }
+    __syncthreads();
+    // half_factors (cpu.rs:265-277): A at offset 0, B at h.
+    for (int p = threadIdx.x; p < H; p += nt) {
+        const int q = p < 2 ? p : (3 << (31 - __clz(p))) - 1 - p;
+        {
+            const F2 sp = s2[swz(H + p)], sq = s2[swz(H + q)];
+            const F2 nx = p == 0 ? f2(sp.re, 0) : sp, ny = p == 0 ? f2(sp.im, 0) : cconj(sq);
+            const F2 iu = f2(u2[H + p].re, u2[H + p].im), iiu = mul_i(iu);
+            const F2 X = cmul(nx, f2(add2(1, iiu.re), iiu.im)), Y = cmul(ny, f2(sub2(1, iiu.re), sub2(0, iiu.im)));
+            ab2[p] = cadd(X, Y);
+            ab2[H + p] = cmul(mul_mi(csub(X, Y)), f2(u2[p].re, u2[p].im));
+        }
+        {
+            const F1 sp = s1[swz(H + p)], sq = s1[swz(H + q)];
+            const F1 nx = p == 0 ? f1(sp.re, 0) : sp, ny = p == 0 ? f1(sp.im, 0) : cconj(sq);
+            const F1 iu = u1[H + p], iiu = mul_i(iu);
+            const F1 X = cmul(nx, f1(add1(1, iiu.re), iiu.im)), Y = cmul(ny, f1(sub1(1, iiu.re), sub1(0, iiu.im)));
+            ab1[p] = cadd(X, Y);
+            ab1[H + p] = cmul(mul_mi(csub(X, Y)), u1[p]);
         }
     }
     __syncthreads();
@@ -195,58 +259,11 @@ __global__ void __launch_bounds__(NT) setup_kernel(const uint32_t* nl, const uin
     fwd_limbs<M, NT>(np, N, s2, s1, tab2, tab1);
     fused_mid<M, NT, false>(np, N, s2, s1, tab2, tab1, SpecStoreOp<M>{o2, o1});
     __syncthreads();
-    // half_forward (cpu.rs:286-295): z_j = N_2j + i N_2j+1, unweighted DIF of length h.
-    for (int j = threadIdx.x; j < H; j += NT) {
-        const uint32_t v0 = nn[2 * j], v1 = nn[2 * j + 1];
-        F2 z2; z2.re = v0; z2.im = v1;
-        uint32_t r0 = (v0 & P1) + (v0 >> 31), r1 = (v1 & P1) + (v1 >> 31);
-        F1 z1; z1.re = min(r0, r0 - P1); z1.im = min(r1, r1 - P1);
-        s2[swz(j)] = z2;
-        s1[swz(j)] = z1;
-    }
-    __syncthreads();
+    pack_pairs(nn, s2, s1, H, NT);
     const F2K* ht2 = tab2 + lt_half_off(M);
     const F1* ht1 = tab1 + lt_half_off(M);
     dif_unweighted<M - 1, NT>(s2, s1, ht2, ht1);
-    const F2K* u2 = tab2 + lt_unpack_off(M);
-    const F1* u1 = tab1 + lt_unpack_off(M);
-    // half_nhat (cpu.rs:239-249) into elements h..2h.
-    for (int p = threadIdx.x; p < H; p += NT) {
-        const int q = p < 2 ? p : (3 << (31 - __clz(p))) - 1 - p;
-        {
-            const F2 zk = lccanon(s2[swz(p)]), zj = cconj(lccanon(s2[swz(q)]));
-            const F2 e = cadd(zk, zj), wo = cmul(mul_mi(csub(zk, zj)), f2(u2[p].re, u2[p].im));
-            const F2 xx = cadd(e, wo), yy = csub(e, wo);
-            s2[swz(H + p)] = p == 0 ? cadd(cmul(xx, inv8h2), mul_i(cmul(yy, inv8h2))) : cmul(xx, inv8h2);
-        }
-        {
-            const F1 zk = s1[swz(p)], zj = cconj(s1[swz(q)]);
-            const F1 e = cadd(zk, zj), wo = cmul(mul_mi(csub(zk, zj)), u1[p]);
-            const F1 xx = cadd(e, wo), yy = csub(e, wo);
-            s1[swz(H + p)] = p == 0 ? cadd(cmul(xx, inv8h1), mul_i(cmul(yy, inv8h1))) : cmul(xx, inv8h1);
-        }
-    }
-    __syncthreads();
-    // half_factors (cpu.rs:265-277): A at h-offset 0, B at h.
-    for (int p = threadIdx.x; p < H; p += NT) {
-        const int q = p < 2 ? p : (3 << (31 - __clz(p))) - 1 - p;
-        {
-            const F2 sp = s2[swz(H + p)], sq = s2[swz(H + q)];
-            const F2 nx = p == 0 ? f2(sp.re, 0) : sp, ny = p == 0 ? f2(sp.im, 0) : cconj(sq);
-            const F2 iu = f2(u2[H + p].re, u2[H + p].im), iiu = mul_i(iu);
-            const F2 X = cmul(nx, f2(add2(1, iiu.re), iiu.im)), Y = cmul(ny, f2(sub2(1, iiu.re), sub2(0, iiu.im)));
-            o2[N + p] = cadd(X, Y);
-            o2[N + H + p] = cmul(mul_mi(csub(X, Y)), f2(u2[p].re, u2[p].im));
-        }
-        {
-            const F1 sp = s1[swz(H + p)], sq = s1[swz(H + q)];
-            const F1 nx = p == 0 ? f1(sp.re, 0) : sp, ny = p == 0 ? f1(sp.im, 0) : cconj(sq);
-            const F1 iu = u1[H + p], iiu = mul_i(iu);
-            const F1 X = cmul(nx, f1(add1(1, iiu.re), iiu.im)), Y = cmul(ny, f1(sub1(1, iiu.re), sub1(0, iiu.im)));
-            o1[N + p] = cadd(X, Y);
-            o1[N + H + p] = cmul(mul_mi(csub(X, Y)), u1[p]);
-        }
-    }
+    half_factors_block(s2, s1, H, tab2 + lt_unpack_off(M), tab1 + lt_unpack_off(M), o2 + N, o1 + N, inv8h2, inv8h1, NT);
 }
 
 }  // namespace mm

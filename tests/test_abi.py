@@ -38,5 +38,9 @@ def test_limits_without_device():
     n = lib.mm_b200_supported_lengths(None, 0)
     arr = (C.c_size_t * n)()
     lib.mm_b200_supported_lengths(arr, n)
-    assert [int(v) for v in arr] == [1 << e for e in range(3, 15)]
+    # Shared-memory lengths 8 .. 16384, then global mode up to 2^24 (the reference's range).
+    assert [int(v) for v in arr] == [1 << e for e in range(3, 25)]
     assert lib.mm_b200_batch_bytes(10, 16384, 1) > 10 * 60 * 8192
+    # Global mode adds a 24-byte work element per transform position and slot.
+    per_slot = lib.mm_b200_batch_bytes(2, 1 << 16, 1) - lib.mm_b200_batch_bytes(1, 1 << 16, 1)
+    assert per_slot == (4 + 8 + 48 + 24) * (1 << 15) + 4 + 12

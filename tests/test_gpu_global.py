@@ -1,0 +1,101 @@
+"""Global mode (L >= 32768: the vector in device memory, 2,048-element tiles streamed through
+shared memory) against the oracle and GMP, through the C ABI. The reference runs these lengths
+with its global-memory kernels (montmul/src/gpu/mod.rs:455-511) and tests them in
+montmul/tests/gpu.rs (force_global cases, lengths up to 2^17)."""
+import pytest
+
+import common
+from montmul_b200 import ModBatch, MontMulError
+from montmul_b200.gmp import RandState, powm
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def gpu():
+    from montmul_b200 import B200
+    dev = B200()
+    return lambda: dev
+
+
+@pytest.fixture(scope="module")
+def gpu_forced():
+    from montmul_b200 import B200
+    dev = B200(force_global=True)
+    return lambda: dev
+
+
+@pytest.fixture(scope="module")
+def wrap(oracle):
+    return lambda: oracle.OracleBackend.wraparound()
+
+
+@pytest.mark.parametrize("length,steps", [(1 << 15, 12), (1 << 16, 8), (1 << 17, 5), (1 << 18, 3)])
+def test_global_same_raw_as_oracle(gpu, wrap, length, steps):
+    """Global lengths against Cpu::with_wraparound at the top of the bucket, raw limbs."""
+    common.same_raw(gpu, wrap, 16 * length - 4, 3, steps)
+
+
+@pytest.mark.parametrize("bits", [131_068, 262_140])
+def test_forced_global_same_raw_as_shared(gpu, gpu_forced, bits):
+    """force_global at L = 8192 and 16384 (gpu/mod.rs:36-44) gives the shared-memory kernels'
+    raw limbs exactly: the same transform split into global passes and tiles."""
+    common.same_raw(gpu, gpu_forced, bits, 6, 40)
+
+
+def test_forced_global_random_modmul(gpu_forced):
+    common.random_modmul(gpu_forced, 100_000, 6, 100_000, 3)
+
+
+@pytest.mark.parametrize("bits", [300_000, 600_000, 1_500_000])
+def test_global_random_modmul(gpu, bits):
+    """Every step's raw result is x^2 c R^-1 mod N in [0, 2N), checked with GMP."""
+    common.random_modmul(gpu, bits, 4, bits, 3)
+
+
+def test_global_edges(gpu):
+    """x = 0, N, 2N - 1 and N = 2^b - 1 at the top and bottom of the global buckets."""
+    for base in (3, 4):
+        common.edges(gpu, base, max_log_len=17)
+
+
+def test_global_powmod_and_mul(gpu):
+    common.powmod_and_mul(gpu, 400_000, 3)
+
+
+def test_global_long_run(gpu):
+    """Several launches (max_launch_steps = 16) on one batch equal pow_mod."""
+    from montmul_b200 import B200
+    dev = B200(max_launch_steps=16)
+    common.long_run(lambda: dev, 500_000, 3, 40)
+
+
+def test_global_carry_overflow_names_the_slot(gpu):
+    rng = RandState()
+    bits = 500_000
+    moduli = [common.rand_odd(rng, bits), common.rand_odd(rng, bits)]
+    b = ModBatch(gpu(), moduli, 4)
+    k = b.params.k
+    for i in range(2):
+        b.load(i, 1)
+        b.set_exponent(i, 1)
+    import numpy as np
+    be, st = b.backend_and_state()
+    be.load(st, 1, np.full(k, 0xFFFFFFFF, np.uint32))
+    with pytest.raises(MontMulError, match="slot 1"):
+        b.run(1)
+
+
+def test_global_pow_prefix(gpu):
+    """3^e mod N for the top 64 bits e of N - 1, random odd 700,000-bit N (global length 2^16),
+    against GMP."""
+    rng = RandState()
+    moduli = [common.rand_odd(rng, 700_000) for _ in range(2)]
+    exps = [n - 1 for n in moduli]
+    b = ModBatch(gpu(), moduli, 3)
+    assert b.params.len >= 1 << 16
+    b.load_all([1] * 2)
+    b.set_exponents([e >> (e.bit_length() - 64) for e in exps])   # the top 64 bits: a prefix run
+    b.run(64)
+    for i, n in enumerate(moduli):
+        assert b.read(i) == powm(3, exps[i] >> (exps[i].bit_length() - 64), n)
