@@ -116,13 +116,59 @@ uint64_t mm_b200_launches(const mm_b200_batch *b);
  * limbs the caller owns; d_err (optional) receives 0, or 1 when a carry that must vanish did
  * not. The work is enqueued on `stream` (a cudaStream_t; NULL is the legacy default stream)
  * and the call returns without waiting. Intermediates live in a static 256 KiB device array
- * that every GPU loading this library holds until exit; lengths needing more scratch are
- * rejected with MM_ERR_ARG (every length this library builds fits). The first call on each
+ * that every GPU loading this library holds until exit; lengths needing more scratch (the
+ * global-mode lengths, L >= 32768) are rejected with MM_ERR_ARG. The first call on each
  * device looks up that array's device address and sets kernel attributes, so make it before
  * any stream capture. All calls share the array: calls that overlap on the GPU race and must
  * be serialized by the caller. */
 int mm_b200_mul_noalloc(const mm_b200_batch *b, size_t slot, const uint32_t *d_a, const uint32_t *d_b,
                         uint32_t *d_out, uint32_t *d_err, void *stream);
+
+/* ---- Schedules (no counterpart in the reference, whose planner fixes them: gpu/plan.rs:26-60) ----
+ * global: 1 runs the batch in global mode (L >= 8192), 0 with the whole vector in shared memory
+ * (L <= 16384). Shared and global mode compute the same per-slot constants, so a batch may
+ * switch at any time. launch_steps: steps per kernel launch of run (0: the device default).
+ * step_ns: the measured time of one slot-step at full occupancy, which orders the items of a
+ * mixed launch (0: a model of the transform work). The autotuner (montmul_b200.tune) measures
+ * these per length and caches them. */
+typedef struct {
+    int global;
+    int launch_steps;
+    double step_ns;
+} mm_b200_schedule;
+int mm_b200_set_schedule(mm_b200_batch *b, const mm_b200_schedule *s);
+int mm_b200_get_schedule(const mm_b200_batch *b, mm_b200_schedule *s);
+
+/* ---- In-place refill (no counterpart in the reference): a serving loop replaces finished
+ * slots while the others keep their state on the device. ----
+ * set_moduli: new moduli for `count` slots (N and N' rows of k limbs, row r for slots[r]); their
+ * per-slot constants are recomputed on the device. write_slots: x rows (k limbs, Montgomery
+ * form in [0, 2N)) and exponents (ew words per row, MSB first, nbits[r] bits) for the listed
+ * slots, positions reset to 0; x or words may be NULL to keep that part. read_slots: x rows of
+ * the listed slots. All three order themselves after earlier work on the batch, including
+ * mixed launches that cover it. */
+int mm_b200_set_moduli(mm_b200_batch *b, size_t count, const size_t *slots, const uint32_t *n, const uint32_t *nprime);
+int mm_b200_write_slots(mm_b200_batch *b, size_t count, const size_t *slots, const uint32_t *x, const uint32_t *words,
+                        size_t ew, const uint32_t *nbits);
+int mm_b200_read_slots(mm_b200_batch *b, size_t count, const size_t *slots, uint32_t *x);
+
+/* ---- Mixed-length persistent launch (no counterpart in the reference) ----
+ * A plan covers every slot of `count` batches on one device, of any lengths. plan_run runs up
+ * to `bits` steps on every slot with bits left, like run on each batch, but in persistent
+ * launches of 256-thread blocks (two per SM) that take (batch, slot) items from a device work
+ * queue, longest first; each launch covers `quantum` steps and is replayed from a CUDA graph.
+ * Batches of L <= 8192 run with the vector in shared memory, longer ones in global mode. The
+ * batches must outlive the plan; plan_sync performs run's error check on every batch. */
+typedef struct mm_b200_plan mm_b200_plan;
+int mm_b200_plan_create(mm_b200_batch *const *batches, size_t count, size_t quantum, mm_b200_plan **out);
+int mm_b200_plan_run_async(mm_b200_plan *p, size_t bits);
+int mm_b200_plan_sync(mm_b200_plan *p);
+int mm_b200_plan_run(mm_b200_plan *p, size_t bits);
+void *mm_b200_plan_stream(mm_b200_plan *p);
+/* Kernel launches of the plan so far, and how many of them were graph replays. */
+uint64_t mm_b200_plan_launches(const mm_b200_plan *p);
+uint64_t mm_b200_plan_graph_launches(const mm_b200_plan *p);
+void mm_b200_plan_destroy(mm_b200_plan *p);
 
 /* Integer roofline probe (no counterpart in the reference, whose roofline is not measured):
  * the peak rate of butterfly pairs (a GF(p^2) product, an add and a sub in both fields) of the

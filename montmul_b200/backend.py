@@ -62,7 +62,29 @@ SIGNATURES = {
     "mm_b200_launches": ([_vp], C.c_uint64),
     "mm_b200_mul_noalloc": ([_vp, _sz, _vp, _vp, _vp, _vp, _vp], C.c_int),
     "mm_b200_bfly_peak": ([C.c_int, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)], C.c_int),
+    "mm_b200_set_schedule": ([_vp, _vp], C.c_int),
+    "mm_b200_get_schedule": ([_vp, _vp], C.c_int),
+    "mm_b200_set_moduli": ([_vp, _sz, _vp, _vp, _vp], C.c_int),
+    "mm_b200_write_slots": ([_vp, _sz, _vp, _vp, _vp, _sz, _vp], C.c_int),
+    "mm_b200_read_slots": ([_vp, _sz, _vp, _vp], C.c_int),
+    "mm_b200_plan_create": ([_vp, _sz, _sz, C.POINTER(_vp)], C.c_int),
+    "mm_b200_plan_run_async": ([_vp, _sz], C.c_int),
+    "mm_b200_plan_sync": ([_vp], C.c_int),
+    "mm_b200_plan_run": ([_vp, _sz], C.c_int),
+    "mm_b200_plan_stream": ([_vp], _vp),
+    "mm_b200_plan_launches": ([_vp], C.c_uint64),
+    "mm_b200_plan_graph_launches": ([_vp], C.c_uint64),
+    "mm_b200_plan_destroy": ([_vp], None),
 }
+
+
+class Schedule(C.Structure):
+    """mm_b200_schedule: global mode, steps per launch, measured ns per slot-step."""
+    _fields_ = [("global_", C.c_int), ("launch_steps", C.c_int), ("step_ns", C.c_double)]
+
+
+def _ptr(a):
+    return a.ctypes.data_as(_vp) if a is not None else None
 
 _lib = None
 
@@ -205,3 +227,76 @@ class B200:
 
     def remaining(self, st, i):
         return int(lib().mm_b200_remaining(st.ptr, i))
+
+    # Schedules and in-place refill (no counterpart in the reference's Backend trait).
+    def set_schedule(self, st, global_mode: bool, launch_steps: int = 0, step_ns: float = 0.0):
+        sc = Schedule(int(global_mode), int(launch_steps), float(step_ns))
+        _check(lib().mm_b200_set_schedule(st.ptr, C.byref(sc)))
+
+    def get_schedule(self, st):
+        sc = Schedule()
+        _check(lib().mm_b200_get_schedule(st.ptr, C.byref(sc)))
+        return {"global": bool(sc.global_), "launch_steps": sc.launch_steps, "step_ns": sc.step_ns}
+
+    def set_moduli(self, st, slots, n, nprime):
+        ids = np.ascontiguousarray(slots, np.uintp)
+        n = np.ascontiguousarray(n, np.uint32)
+        nprime = np.ascontiguousarray(nprime, np.uint32)
+        assert n.shape == nprime.shape == (len(ids), st.k)
+        _check(lib().mm_b200_set_moduli(st.ptr, len(ids), _ptr(ids), _ptr(n), _ptr(nprime)))
+
+    def write_slots(self, st, slots, x=None, words=None, nbits=None):
+        ids = np.ascontiguousarray(slots, np.uintp)
+        xa = None if x is None else np.ascontiguousarray(x, np.uint32)
+        wa = None if words is None else np.ascontiguousarray(words, np.uint32)
+        nb = None if nbits is None else np.ascontiguousarray(nbits, np.uint32)
+        if xa is not None:
+            assert xa.shape == (len(ids), st.k)
+        ew = 0 if wa is None else wa.shape[1]
+        _check(lib().mm_b200_write_slots(st.ptr, len(ids), _ptr(ids), _ptr(xa), _ptr(wa), ew, _ptr(nb)))
+
+    def read_slots(self, st, slots):
+        ids = np.ascontiguousarray(slots, np.uintp)
+        o = np.zeros((len(ids), st.k), np.uint32)
+        _check(lib().mm_b200_read_slots(st.ptr, len(ids), _ptr(ids), _ptr(o)))
+        return o
+
+
+class Plan:
+    """A mixed-length persistent launch over every slot of several batches on one device
+    (mm_b200_plan_*): `run(bits)` advances every slot like ModBatch.run on each batch, in
+    launches of `quantum` steps replayed from a CUDA graph. The batches must outlive the plan."""
+
+    def __init__(self, batches, quantum: int = 1 << 16):
+        states = [b.backend_and_state()[1] if hasattr(b, "backend_and_state") else b for b in batches]
+        arr = (_vp * len(states))(*[s.ptr for s in states])
+        ptr = _vp()
+        _check(lib().mm_b200_plan_create(arr, len(states), int(quantum), C.byref(ptr)))
+        self._p = ptr
+        self._keep = list(batches)
+
+    def run(self, bits: int) -> None:
+        _check(lib().mm_b200_plan_run(self._p, int(bits)))
+
+    def run_async(self, bits: int) -> None:
+        _check(lib().mm_b200_plan_run_async(self._p, int(bits)))
+
+    def sync(self) -> None:
+        _check(lib().mm_b200_plan_sync(self._p))
+
+    def stream(self) -> int:
+        return int(lib().mm_b200_plan_stream(self._p) or 0)
+
+    def launches(self) -> int:
+        return int(lib().mm_b200_plan_launches(self._p))
+
+    def graph_launches(self) -> int:
+        return int(lib().mm_b200_plan_graph_launches(self._p))
+
+    def close(self) -> None:
+        if getattr(self, "_p", None):
+            lib().mm_b200_plan_destroy(self._p)
+            self._p = None
+
+    def __del__(self):
+        self.close()

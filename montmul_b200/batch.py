@@ -201,6 +201,36 @@ class ModBatch:
         m = self.moduli[i]
         return gmp.mulmod(self.read_raw(i), m.rinv, m.n)
 
+    def refill(self, slots, moduli, xs, exps) -> None:
+        """Replaces the moduli of `slots` and loads x and an exponent into each, the other slots
+        keeping their state on the device (a serving loop's in-place refill; no counterpart in
+        the reference). Every new modulus must fit this batch's length and limb count."""
+        slots = [int(i) for i in slots]
+        moduli = [int(n) for n in moduli]
+        k = self.params.k
+        for n in moduli:
+            if n <= 1 or n % 2 == 0:
+                raise MontMulError("modulus must be odd and > 1")
+            if Params.for_bits(n.bit_length(), self.backend.supported_lengths()).len > self.params.len or \
+                    n.bit_length() + 4 > 32 * k:
+                raise MontMulError("modulus does not fit this batch's length")
+        per = [_setup_one(n, k) for n in moduli]
+        self.backend.set_moduli(self.state, slots, np.stack([p[0] for p in per]), np.stack([p[1] for p in per]))
+        for i, p in zip(slots, per):
+            self.moduli[i] = p[3]
+        x = np.stack([to_limbs(self._mont(i, int(v)), k) for i, v in zip(slots, xs)])
+        ws = [exponent_words(int(e)) for e in exps]
+        ew = max(1, max(len(w) for w, _ in ws))
+        words = np.zeros((len(ws), ew), np.uint32)
+        for r, (w, _) in enumerate(ws):
+            words[r, : len(w)] = w
+        self.backend.write_slots(self.state, slots, x, words, np.array([nb for _, nb in ws], np.uint32))
+
+    def read_raw_slots(self, slots):
+        """Raw Montgomery-form values of several slots with one device read."""
+        rows = self.backend.read_slots(self.state, [int(i) for i in slots])
+        return [from_limbs(r) for r in rows]
+
     def is_one(self, i: int) -> bool:
         """True if slot i holds 1: raw R mod N or R mod N + N (batch.rs:179-183)."""
         m = self.moduli[i]

@@ -24,7 +24,8 @@ struct SlotArgs {
 
 typedef void (*StepFn)(SlotArgs, uint32_t, uint32_t);
 typedef void (*MulFn)(SlotArgs, uint32_t, uint32_t, uint32_t, F2*, F1*);
-typedef void (*SetupFn)(const uint32_t*, const uint32_t*, F2*, F1*, const F2K*, const F1*, F2, F1, uint32_t);
+typedef void (*SetupFn)(const uint32_t*, const uint32_t*, F2*, F1*, const F2K*, const F1*, F2, F1, uint32_t,
+                        const uint32_t*);
 
 struct KernelSet {
     StepFn step;
@@ -44,7 +45,7 @@ struct GArgs {
 };
 typedef void (*GStepFn)(GArgs, uint32_t, uint32_t);
 typedef void (*GMulFn)(GArgs, uint32_t, uint32_t, uint32_t, F2*, F1*);
-typedef void (*GSetupFn)(GArgs, const uint32_t*, const uint32_t*, F2*, F1*, F2, F1, uint32_t);
+typedef void (*GSetupFn)(GArgs, const uint32_t*, const uint32_t*, F2*, F1*, F2, F1, uint32_t, const uint32_t*);
 struct GlobalKernels {
     GStepFn step;
     GMulFn mul;
@@ -54,6 +55,19 @@ struct GlobalKernels {
 };
 constexpr int kMinGlobalLogN = 12;   // smallest length the global kernels accept (one tile per half)
 GlobalKernels global_kernels();       // mm_global.cu
+
+// The mixed-length persistent launch (mm_mixed.cu): one descriptor per batch, one work item
+// (descriptor index, slot) per slot; blocks take items from a device counter in item order.
+struct MixedDesc {
+    GArgs g;       // the batch's slot state (w2 / w1 unused in shared mode)
+    int global;    // 1: global mode; 0: the vector in shared memory (m <= kMaxMixedSharedLogN)
+    int pad;
+};
+constexpr int kMixedThreads = 256;
+constexpr int kMaxMixedSharedLogN = 12;   // 96 KiB: two blocks per SM, as global mode
+constexpr int kMixedSmem = 24 << kMaxMixedSharedLogN;
+typedef void (*MixedFn)(const MixedDesc*, const uint2*, uint32_t, uint32_t*, uint32_t);
+MixedFn mixed_kernel();               // mm_mixed.cu
 
 // Threads per block for transform length 2^m: one radix-8 group per thread up to 256 threads.
 constexpr int threads_for(int m) { return m - 3 <= 5 ? 32 : (m - 3 >= 8 ? 256 : (1 << (m - 3))); }

@@ -73,6 +73,7 @@ struct mm_b200_device {
     int max_launch_steps = 512;
     bool force_global = false;
     bool global_configured = false;
+    bool mixed_configured = false;
     std::string name;
     std::mutex mu;
     std::map<int, DevTables> tables;
@@ -89,6 +90,12 @@ struct mm_b200_batch {
     GlobalKernels gk{};
     F2* d_w2 = nullptr;        // global mode: slots x n work elements
     F1* d_w1 = nullptr;
+    const DevTables* gtab = nullptr;   // global-mode tables (global batches; L = 16384 in a mixed plan)
+    mm_b200_schedule sched{0, 0, 0.0};
+    uint32_t* d_stage = nullptr;       // refill staging: device words and pinned host words
+    size_t stage_cap = 0;
+    uint32_t* h_stage = nullptr;
+    size_t hstage_cap = 0;
     cudaStream_t stream = nullptr;
     uint32_t* d_x = nullptr;
     uint32_t* d_t = nullptr;
@@ -175,9 +182,12 @@ SlotArgs slot_args(const mm_b200_batch* b) {
     return a;
 }
 
+// Requires the batch's global-mode tables (a global batch, or ensure_global_buffers).
 GArgs global_args(const mm_b200_batch* b) {
     GArgs g;
     g.a = slot_args(b);
+    g.a.tab2 = b->gtab->t2;
+    g.a.tab1 = b->gtab->t1;
     g.w2 = b->d_w2;
     g.w1 = b->d_w1;
     g.m = b->m;
@@ -256,8 +266,9 @@ int launch_steps(mm_b200_batch* b, size_t bits) {
     int rc = push(b);
     if (rc) return rc;
     const SlotArgs a = slot_args(b);
-    const GArgs g = global_args(b);
-    const size_t chunk = (size_t)std::max(1, b->dev->max_launch_steps);
+    GArgs g{};
+    if (b->global) g = global_args(b);
+    const size_t chunk = (size_t)std::max(1, b->sched.launch_steps > 0 ? b->sched.launch_steps : b->dev->max_launch_steps);
     while (left > 0) {
         const uint32_t s = (uint32_t)std::min(left, chunk);
         if (b->global) b->gk.step<<<(unsigned)b->slots, b->gk.threads, b->gk.smem, b->stream>>>(g, 0, s);
@@ -268,6 +279,91 @@ int launch_steps(mm_b200_batch* b, size_t bits) {
         left -= s;
     }
     b->host_x_valid = false;
+    return MM_OK;
+}
+
+// Global-mode work vectors and tables for a batch created in shared mode (a schedule switch, or
+// L = 16384 in a mixed plan, whose blocks have 96 KiB of shared memory).
+int ensure_global_buffers(mm_b200_batch* b) {
+    if (b->m < kMinGlobalLogN) return fail(MM_ERR_UNSUPPORTED, "global mode needs L >= 8192");
+    if (!b->gtab) {
+        const DevTables* t = nullptr;
+        int rc = ensure_tables(b->dev, b->m, true, &t);
+        if (rc) return rc;
+        b->gtab = t;
+    }
+    if (!b->d_w2) {
+        MM_CK(cudaMalloc(&b->d_w2, b->slots * b->n * sizeof(F2)));
+        MM_CK(cudaMalloc(&b->d_w1, b->slots * b->n * sizeof(F1)));
+    }
+    return MM_OK;
+}
+
+// Staging words for a refill: pinned host and device buffers of at least `words` u32. Waits
+// for the batch's stream first, since an earlier copy may still read the pinned buffer.
+int ensure_stage(mm_b200_batch* b, size_t words) {
+    MM_CK(cudaStreamSynchronize(b->stream));
+    if (words > b->stage_cap) {
+        if (b->d_stage) MM_CK(cudaFree(b->d_stage));
+        b->d_stage = nullptr;
+        MM_CK(cudaMalloc(&b->d_stage, words * 4));
+        b->stage_cap = words;
+    }
+    if (words > b->hstage_cap) {
+        if (b->h_stage) MM_CK(cudaFreeHost(b->h_stage));
+        b->h_stage = nullptr;
+        MM_CK(cudaMallocHost(&b->h_stage, words * 4));
+        b->hstage_cap = words;
+    }
+    return MM_OK;
+}
+
+// Widens the device exponent rows to `ew` words per slot, keeping every row.
+int grow_exponents(mm_b200_batch* b, size_t ew) {
+    uint32_t* nd = nullptr;
+    MM_CK(cudaMalloc(&nd, b->slots * ew * 4));
+    MM_CK(cudaMemsetAsync(nd, 0, b->slots * ew * 4, b->stream));
+    MM_CK(cudaMemcpy2DAsync(nd, ew * 4, b->d_exp, b->ew * 4, b->ew * 4, b->slots, cudaMemcpyDeviceToDevice, b->stream));
+    MM_CK(cudaStreamSynchronize(b->stream));
+    MM_CK(cudaFree(b->d_exp));
+    b->d_exp = nd;
+    b->exp_cap = ew;
+    b->ew = ew;
+    return MM_OK;
+}
+
+// Refill scatter: stage = [slot ids | nbits | x rows (k) | exponent rows (ew_in)], one block per
+// row; exponent rows are zero-padded to the batch's row stride ew_out.
+__global__ void scatter_rows_kernel(const uint32_t* __restrict__ stage, uint32_t count, uint32_t k, uint32_t ew_in,
+                                    uint32_t ew_out, uint32_t* x, uint32_t* exp, uint32_t* nbits, uint32_t* pos) {
+    const uint32_t r = blockIdx.x;
+    const size_t slot = stage[r];
+    const uint32_t* xs = stage + 2 * (size_t)count + (size_t)r * k;
+    const uint32_t* es = stage + 2 * (size_t)count + (size_t)count * k + (size_t)r * ew_in;
+    if (x)
+        for (uint32_t j = threadIdx.x; j < k; j += blockDim.x) x[slot * k + j] = xs[j];
+    if (exp) {
+        for (uint32_t j = threadIdx.x; j < ew_out; j += blockDim.x) exp[slot * ew_out + j] = j < ew_in ? es[j] : 0u;
+        if (threadIdx.x == 0) {
+            nbits[slot] = stage[count + r];
+            pos[slot] = 0;
+        }
+    }
+}
+
+// Refill gather: x rows of the slots listed in stage[0 .. count) into out (count x k).
+__global__ void gather_rows_kernel(const uint32_t* __restrict__ ids, uint32_t k, const uint32_t* __restrict__ x,
+                                   uint32_t* out) {
+    const uint32_t r = blockIdx.x;
+    const size_t slot = ids[r];
+    for (uint32_t j = threadIdx.x; j < k; j += blockDim.x) out[(size_t)r * k + j] = x[slot * k + j];
+}
+
+int check_slot_list(const mm_b200_batch* b, size_t count, const size_t* slots, const char* what) {
+    if (!slots && count) return fail(MM_ERR_ARG, std::string(what) + ": null slot list");
+    if (count > 0xffffffffu) return fail(MM_ERR_ARG, std::string(what) + ": too many slots");
+    for (size_t r = 0; r < count; ++r)
+        if (slots[r] >= b->slots) return fail(MM_ERR_ARG, std::string(what) + ": bad slot " + std::to_string(slots[r]));
     return MM_OK;
 }
 
@@ -384,9 +480,14 @@ int mm_b200_create(mm_b200_device* dev, size_t k, size_t len, uint32_t base, siz
     const size_t need = mm_b200_batch_bytes(slots, len, 1) + 8 * slots * k + forced + ((size_t)64 << 20);
     const size_t freeb = mm_b200_free_memory(dev);
     if (need > freeb) return fail(MM_ERR_OOM, "batch needs " + std::to_string(need) + " bytes, " + std::to_string(freeb) + " free");
-    const DevTables* tab = nullptr;
-    int rc = ensure_tables(dev, m, global, &tab);
+    // Shared-mode tables for every length that has them (mul_noalloc and schedule switches read
+    // them), global-mode tables for a global batch.
+    const DevTables *stab = nullptr, *gtab = nullptr;
+    int rc = MM_OK;
+    if (m <= kMaxSharedLogN) rc = ensure_tables(dev, m, false, &stab);
+    if (!rc && global) rc = ensure_tables(dev, m, true, &gtab);
     if (rc) return rc;
+    const DevTables* tab = stab ? stab : gtab;
     // On a failure below, everything allocated so far is released with the batch.
     std::unique_ptr<mm_b200_batch, void (*)(mm_b200_batch*)> b(new mm_b200_batch(), mm_b200_destroy);
     b->dev = dev;
@@ -397,8 +498,10 @@ int mm_b200_create(mm_b200_device* dev, size_t k, size_t len, uint32_t base, siz
     b->base = base;
     b->tab = tab;
     b->global = global;
-    if (global) b->gk = global_kernels();
-    else kernel_set(m, b->ks);
+    b->sched.global = global ? 1 : 0;
+    b->gk = global_kernels();
+    b->gtab = gtab;
+    if (m <= kMaxSharedLogN) kernel_set(m, b->ks);
     MM_CK(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
     const size_t nn = b->n;
     MM_CK(cudaMalloc(&b->d_x, slots * k * 4));
@@ -432,10 +535,10 @@ int mm_b200_create(mm_b200_device* dev, size_t k, size_t len, uint32_t base, siz
         const unsigned grid = (unsigned)std::min<size_t>(65535, slots - first);
         if (global)
             b->gk.setup<<<grid, b->gk.threads, b->gk.smem, b->stream>>>(global_args(b.get()), d_n, d_np, b->d_c2, b->d_c1,
-                                                                       tab->inv8h2, tab->inv8h1, (uint32_t)first);
+                                                                       gtab->inv8h2, gtab->inv8h1, (uint32_t)first, nullptr);
         else
             b->ks.setup<<<grid, b->ks.threads, b->ks.smem, b->stream>>>(d_n, d_np, b->d_c2, b->d_c1, tab->t2, tab->t1,
-                                                                       tab->inv8h2, tab->inv8h1, (uint32_t)first);
+                                                                       tab->inv8h2, tab->inv8h1, (uint32_t)first, nullptr);
         MM_CK(cudaGetLastError());
         ++b->launches;
     }
@@ -582,10 +685,346 @@ void mm_b200_destroy(mm_b200_batch* b) {
     cudaFree(b->d_spec1);
     cudaFree(b->d_w2);
     cudaFree(b->d_w1);
+    cudaFree(b->d_stage);
+    if (b->h_stage) cudaFreeHost(b->h_stage);
     if (b->stream) cudaStreamDestroy(b->stream);
     if (b->host_x) cudaFreeHost(b->host_x);
     if (b->host_exp) cudaFreeHost(b->host_exp);
     delete b;
+}
+
+int mm_b200_set_schedule(mm_b200_batch* b, const mm_b200_schedule* sc) {
+    if (!b || !sc) return fail(MM_ERR_ARG, "set_schedule: null argument");
+    if (sc->launch_steps < 0 || sc->step_ns < 0) return fail(MM_ERR_ARG, "set_schedule: negative value");
+    MM_CK(cudaSetDevice(b->dev->device));
+    const bool global = sc->global != 0;
+    if (!global && b->m > kMaxSharedLogN) return fail(MM_ERR_UNSUPPORTED, "set_schedule: L > 16384 runs in global mode only");
+    if (global) {
+        int rc = ensure_global_buffers(b);
+        if (rc) return rc;
+    }
+    b->global = global;
+    b->sched = *sc;
+    b->sched.global = global ? 1 : 0;
+    return MM_OK;
+}
+
+int mm_b200_get_schedule(const mm_b200_batch* b, mm_b200_schedule* sc) {
+    if (!b || !sc) return fail(MM_ERR_ARG, "get_schedule: null argument");
+    *sc = b->sched;
+    return MM_OK;
+}
+
+int mm_b200_set_moduli(mm_b200_batch* b, size_t count, const size_t* slots, const uint32_t* n, const uint32_t* nprime) {
+    if (!b || ((!n || !nprime) && count)) return fail(MM_ERR_ARG, "set_moduli: null argument");
+    int rc = check_slot_list(b, count, slots, "set_moduli");
+    if (rc || count == 0) return rc;
+    MM_CK(cudaSetDevice(b->dev->device));
+    const size_t k = b->k;
+    rc = ensure_stage(b, count * (1 + 2 * k));
+    if (rc) return rc;
+    uint32_t* h = b->h_stage;
+    for (size_t r = 0; r < count; ++r) h[r] = (uint32_t)slots[r];
+    std::memcpy(h + count, n, count * k * 4);
+    std::memcpy(h + count + count * k, nprime, count * k * 4);
+    MM_CK(cudaMemcpyAsync(b->d_stage, h, count * (1 + 2 * k) * 4, cudaMemcpyHostToDevice, b->stream));
+    const DevTables* tab = b->global ? b->gtab : b->tab;
+    for (size_t c0 = 0; c0 < count; c0 += 65535) {
+        const unsigned grid = (unsigned)std::min<size_t>(65535, count - c0);
+        const uint32_t* ids = b->d_stage + c0;
+        const uint32_t* nl = b->d_stage + count + c0 * k;
+        const uint32_t* npl = b->d_stage + count + count * k + c0 * k;
+        if (b->global)
+            b->gk.setup<<<grid, b->gk.threads, b->gk.smem, b->stream>>>(global_args(b), nl, npl, b->d_c2, b->d_c1,
+                                                                       tab->inv8h2, tab->inv8h1, 0, ids);
+        else
+            b->ks.setup<<<grid, b->ks.threads, b->ks.smem, b->stream>>>(nl, npl, b->d_c2, b->d_c1, tab->t2, tab->t1,
+                                                                       tab->inv8h2, tab->inv8h1, 0, ids);
+        MM_CK(cudaGetLastError());
+        ++b->launches;
+    }
+    return MM_OK;
+}
+
+int mm_b200_write_slots(mm_b200_batch* b, size_t count, const size_t* slots, const uint32_t* x, const uint32_t* words,
+                        size_t ew, const uint32_t* nbits) {
+    if (!b) return fail(MM_ERR_ARG, "write_slots: null batch");
+    int rc = check_slot_list(b, count, slots, "write_slots");
+    if (rc || count == 0) return rc;
+    if (words && (!nbits || ew == 0)) return fail(MM_ERR_ARG, "write_slots: exponents need ew > 0 and nbits");
+    if (words)
+        for (size_t r = 0; r < count; ++r)
+            if (nbits[r] > 32 * ew) return fail(MM_ERR_ARG, "write_slots: nbits exceeds the words");
+    MM_CK(cudaSetDevice(b->dev->device));
+    // Earlier host-side loads and exponents reach the device first.
+    rc = push(b);
+    if (rc) return rc;
+    if (words && ew > b->ew) {
+        rc = grow_exponents(b, ew);
+        if (rc) return rc;
+    }
+    const size_t k = b->k, ewi = words ? ew : 0;
+    const size_t total = count * (2 + k + ewi);
+    rc = ensure_stage(b, total);
+    if (rc) return rc;
+    uint32_t* h = b->h_stage;
+    for (size_t r = 0; r < count; ++r) {
+        h[r] = (uint32_t)slots[r];
+        h[count + r] = words ? nbits[r] : 0;
+    }
+    if (x) std::memcpy(h + 2 * count, x, count * k * 4);
+    if (words) std::memcpy(h + 2 * count + count * k, words, count * ew * 4);
+    MM_CK(cudaMemcpyAsync(b->d_stage, h, total * 4, cudaMemcpyHostToDevice, b->stream));
+    scatter_rows_kernel<<<(unsigned)count, 128, 0, b->stream>>>(b->d_stage, (uint32_t)count, (uint32_t)k, (uint32_t)ewi,
+                                                                (uint32_t)b->ew, x ? b->d_x : nullptr,
+                                                                words ? b->d_exp : nullptr, b->d_nbits, b->d_pos);
+    MM_CK(cudaGetLastError());
+    for (size_t r = 0; r < count; ++r) {
+        const size_t i = slots[r];
+        if (x && b->host_x_valid) std::memcpy(b->host_x + i * k, x + r * k, k * 4);
+        if (words) {
+            b->exps[i].assign(words + r * ew, words + (r + 1) * ew);
+            b->nbits[i] = nbits[r];
+            b->pos[i] = 0;
+        }
+    }
+    return MM_OK;
+}
+
+int mm_b200_read_slots(mm_b200_batch* b, size_t count, const size_t* slots, uint32_t* x) {
+    if (!b || (!x && count)) return fail(MM_ERR_ARG, "read_slots: null argument");
+    int rc = check_slot_list(b, count, slots, "read_slots");
+    if (rc || count == 0) return rc;
+    const size_t k = b->k;
+    if (b->host_x_valid) {
+        for (size_t r = 0; r < count; ++r) std::memcpy(x + r * k, b->host_x + slots[r] * k, k * 4);
+        return MM_OK;
+    }
+    MM_CK(cudaSetDevice(b->dev->device));
+    rc = ensure_stage(b, count * (1 + k));
+    if (rc) return rc;
+    uint32_t* h = b->h_stage;
+    for (size_t r = 0; r < count; ++r) h[r] = (uint32_t)slots[r];
+    MM_CK(cudaMemcpyAsync(b->d_stage, h, count * 4, cudaMemcpyHostToDevice, b->stream));
+    gather_rows_kernel<<<(unsigned)count, 128, 0, b->stream>>>(b->d_stage, (uint32_t)k, b->d_x, b->d_stage + count);
+    MM_CK(cudaGetLastError());
+    MM_CK(cudaMemcpyAsync(h + count, b->d_stage + count, count * k * 4, cudaMemcpyDeviceToHost, b->stream));
+    MM_CK(cudaStreamSynchronize(b->stream));
+    std::memcpy(x, h + count, count * k * 4);
+    return MM_OK;
+}
+
+}  // extern "C"
+
+// ---- the mixed-length plan ----
+struct mm_b200_plan {
+    mm_b200_device* dev = nullptr;
+    std::vector<mm_b200_batch*> batches;
+    std::vector<cudaEvent_t> ready;   // per batch: its stream's work before a launch
+    cudaEvent_t done = nullptr;       // the plan's last launch
+    cudaStream_t stream = nullptr;
+    size_t quantum = 0;
+    int grid = 0;
+    MixedDesc* d_descs = nullptr;
+    MixedDesc* h_descs = nullptr;     // pinned copy of what the device holds
+    uint2* d_items = nullptr;
+    uint32_t count = 0;
+    uint32_t* d_counter = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    uint64_t launches = 0, graph_launches = 0;
+};
+
+namespace {
+
+// Relative cost of one slot-step of a batch: the schedule's measured time, else the transform
+// work n log2 n (global mode pays about a fifth more in memory traffic).
+double step_cost(const mm_b200_batch* b, bool global) {
+    if (b->sched.step_ns > 0) return b->sched.step_ns;
+    const double n = (double)b->n;
+    return n * (double)b->m * (global ? 1.2 : 1.0);
+}
+
+MixedDesc mixed_desc(const mm_b200_batch* b, bool global) {
+    MixedDesc d{};
+    if (global) d.g = global_args(b);
+    else {
+        d.g.a = slot_args(b);
+        d.g.w2 = nullptr;
+        d.g.w1 = nullptr;
+        d.g.m = b->m;
+    }
+    d.global = global ? 1 : 0;
+    return d;
+}
+
+bool plan_global(const mm_b200_batch* b) { return b->global || b->m > kMaxMixedSharedLogN; }
+
+// One launch of `bits` steps: the counter reset and the persistent kernel.
+int plan_enqueue(mm_b200_plan* p, uint32_t bits) {
+    MM_CK(cudaMemsetAsync(p->d_counter, 0, 4, p->stream));
+    mixed_kernel()<<<p->grid, kMixedThreads, kMixedSmem, p->stream>>>(p->d_descs, p->d_items, p->count, p->d_counter, bits);
+    MM_CK(cudaGetLastError());
+    return MM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int mm_b200_plan_create(mm_b200_batch* const* batches, size_t count, size_t quantum, mm_b200_plan** out) {
+    if (!batches || !out || count == 0) return fail(MM_ERR_ARG, "plan_create: no batches");
+    if (quantum == 0 || quantum > 0xffffffffu) return fail(MM_ERR_ARG, "plan_create: quantum must be in 1 .. 2^32 - 1");
+    mm_b200_device* dev = batches[0] ? batches[0]->dev : nullptr;
+    size_t total = 0;
+    for (size_t i = 0; i < count; ++i) {
+        if (!batches[i]) return fail(MM_ERR_ARG, "plan_create: null batch");
+        if (batches[i]->dev != dev) return fail(MM_ERR_ARG, "plan_create: batches on different devices");
+        total += batches[i]->slots;
+    }
+    if (total > 0xffffffffu) return fail(MM_ERR_ARG, "plan_create: too many slots");
+    MM_CK(cudaSetDevice(dev->device));
+    for (size_t i = 0; i < count; ++i) {
+        if (plan_global(batches[i])) {
+            int rc = ensure_global_buffers(batches[i]);
+            if (rc) return rc;
+        }
+    }
+    std::unique_ptr<mm_b200_plan, void (*)(mm_b200_plan*)> p(new mm_b200_plan(), mm_b200_plan_destroy);
+    p->dev = dev;
+    p->batches.assign(batches, batches + count);
+    p->quantum = quantum;
+    p->count = (uint32_t)total;
+    MM_CK(cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking));
+    MM_CK(cudaEventCreateWithFlags(&p->done, cudaEventDisableTiming));
+    p->ready.assign(count, nullptr);
+    for (auto& e : p->ready) MM_CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    {
+        std::lock_guard<std::mutex> lock(dev->mu);
+        if (!dev->mixed_configured) {
+            MM_CK(cudaFuncSetAttribute((const void*)mixed_kernel(), cudaFuncAttributeMaxDynamicSharedMemorySize, kMixedSmem));
+            MM_CK(cudaFuncSetAttribute((const void*)mixed_kernel(), cudaFuncAttributePreferredSharedMemoryCarveout,
+                                       cudaSharedmemCarveoutMaxShared));
+            dev->mixed_configured = true;
+        }
+    }
+    int per_sm = 0;
+    MM_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, mixed_kernel(), kMixedThreads, kMixedSmem));
+    p->grid = std::max(1, per_sm) * dev->sms;
+    // Items longest first (by cost per step; every slot of a batch has the same), then by batch
+    // and slot.
+    std::vector<std::pair<double, uint2>> items;
+    items.reserve(total);
+    for (size_t i = 0; i < count; ++i) {
+        const double c = step_cost(batches[i], plan_global(batches[i]));
+        for (size_t s = 0; s < batches[i]->slots; ++s) items.push_back({c, make_uint2((unsigned)i, (unsigned)s)});
+    }
+    std::stable_sort(items.begin(), items.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
+    std::vector<uint2> it(total);
+    for (size_t i = 0; i < total; ++i) it[i] = items[i].second;
+    MM_CK(cudaMalloc(&p->d_items, total * sizeof(uint2)));
+    MM_CK(cudaMemcpy(p->d_items, it.data(), total * sizeof(uint2), cudaMemcpyHostToDevice));
+    MM_CK(cudaMalloc(&p->d_descs, count * sizeof(MixedDesc)));
+    MM_CK(cudaMallocHost(&p->h_descs, count * sizeof(MixedDesc)));
+    std::memset(p->h_descs, 0, count * sizeof(MixedDesc));
+    MM_CK(cudaMalloc(&p->d_counter, 4));
+    *out = p.release();
+    return MM_OK;
+}
+
+int mm_b200_plan_run_async(mm_b200_plan* p, size_t bits) {
+    if (!p) return fail(MM_ERR_ARG, "plan_run: null plan");
+    MM_CK(cudaSetDevice(p->dev->device));
+    size_t most = 0;
+    for (auto* b : p->batches)
+        for (size_t i = 0; i < b->slots; ++i) most = std::max(most, (size_t)(b->nbits[i] - b->pos[i]));
+    size_t left = std::min(bits, most);
+    if (left == 0) return MM_OK;
+    const size_t nb = p->batches.size();
+    for (size_t i = 0; i < nb; ++i) {
+        mm_b200_batch* b = p->batches[i];
+        int rc = push(b);
+        if (rc) return rc;
+        MM_CK(cudaEventRecord(p->ready[i], b->stream));
+        MM_CK(cudaStreamWaitEvent(p->stream, p->ready[i], 0));
+    }
+    // Descriptors follow the batches' buffers (exponent rows can be reallocated and restrided).
+    std::vector<MixedDesc> d(nb);
+    for (size_t i = 0; i < nb; ++i) d[i] = mixed_desc(p->batches[i], plan_global(p->batches[i]));
+    if (std::memcmp(d.data(), p->h_descs, nb * sizeof(MixedDesc)) != 0) {
+        MM_CK(cudaStreamSynchronize(p->stream));   // the pinned copy may still feed the last upload
+        std::memcpy(p->h_descs, d.data(), nb * sizeof(MixedDesc));
+        MM_CK(cudaMemcpyAsync(p->d_descs, p->h_descs, nb * sizeof(MixedDesc), cudaMemcpyHostToDevice, p->stream));
+    }
+    while (left > 0) {
+        const size_t s = std::min(left, p->quantum);
+        if (s == p->quantum) {
+            if (!p->exec) {
+                MM_CK(cudaStreamBeginCapture(p->stream, cudaStreamCaptureModeThreadLocal));
+                int rc = plan_enqueue(p, (uint32_t)s);
+                cudaGraph_t g = nullptr;
+                cudaError_t e = cudaStreamEndCapture(p->stream, &g);
+                if (rc) return rc;
+                if (e != cudaSuccess) return fail(MM_ERR_CUDA, std::string("plan capture: ") + cudaGetErrorString(e));
+                p->graph = g;
+                MM_CK(cudaGraphInstantiate(&p->exec, p->graph, 0));
+            }
+            MM_CK(cudaGraphLaunch(p->exec, p->stream));
+            ++p->graph_launches;
+        } else {
+            int rc = plan_enqueue(p, (uint32_t)s);
+            if (rc) return rc;
+        }
+        ++p->launches;
+        for (auto* b : p->batches) {
+            for (size_t i = 0; i < b->slots; ++i) b->pos[i] += std::min<uint32_t>((uint32_t)s, b->nbits[i] - b->pos[i]);
+        }
+        left -= s;
+    }
+    MM_CK(cudaEventRecord(p->done, p->stream));
+    for (auto* b : p->batches) {
+        MM_CK(cudaStreamWaitEvent(b->stream, p->done, 0));
+        b->host_x_valid = false;
+    }
+    return MM_OK;
+}
+
+int mm_b200_plan_sync(mm_b200_plan* p) {
+    if (!p) return fail(MM_ERR_ARG, "plan_sync: null plan");
+    MM_CK(cudaSetDevice(p->dev->device));
+    MM_CK(cudaStreamSynchronize(p->stream));
+    for (auto* b : p->batches) {
+        int rc = check_err(b, "run");
+        if (rc) return rc;
+    }
+    return MM_OK;
+}
+
+int mm_b200_plan_run(mm_b200_plan* p, size_t bits) {
+    int rc = mm_b200_plan_run_async(p, bits);
+    if (rc) return rc;
+    return mm_b200_plan_sync(p);
+}
+
+void* mm_b200_plan_stream(mm_b200_plan* p) { return p ? (void*)p->stream : nullptr; }
+uint64_t mm_b200_plan_launches(const mm_b200_plan* p) { return p ? p->launches : 0; }
+uint64_t mm_b200_plan_graph_launches(const mm_b200_plan* p) { return p ? p->graph_launches : 0; }
+
+void mm_b200_plan_destroy(mm_b200_plan* p) {
+    if (!p) return;
+    if (p->dev) cudaSetDevice(p->dev->device);
+    if (p->stream) cudaStreamSynchronize(p->stream);
+    if (p->exec) cudaGraphExecDestroy(p->exec);
+    if (p->graph) cudaGraphDestroy(p->graph);
+    cudaFree(p->d_items);
+    cudaFree(p->d_descs);
+    cudaFree(p->d_counter);
+    if (p->h_descs) cudaFreeHost(p->h_descs);
+    for (auto e : p->ready)
+        if (e) cudaEventDestroy(e);
+    if (p->done) cudaEventDestroy(p->done);
+    if (p->stream) cudaStreamDestroy(p->stream);
+    delete p;
 }
 
 }  // extern "C"

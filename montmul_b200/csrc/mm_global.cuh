@@ -454,17 +454,14 @@ __device__ __forceinline__ int g_redc_wrap(F2* w2, F1* w1, int m, const uint32_t
     return g_wrap_combine<NT>(w2, w1, n, tl, x, sc) ? kStepOk : kStepCarry;
 }
 
-// Up to `bits` steps on slot first + blockIdx.x, global mode (as step_kernel).
+// Up to `bits` steps on one slot, global mode (as step_slot). `par` carries the mbarrier
+// parities from one call to the next. Returns false (on every thread) after a bulk copy that did
+// not complete in time; the parities are then no longer usable.
 template <int NT>
-__global__ void __launch_bounds__(NT, 2) gstep_kernel(GArgs g, uint32_t first, uint32_t bits) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ uint64_t sc[CarryScratch<NT>::words];
-    __shared__ uint64_t bars[2];
-    const TileSmem sm{smem_raw, bars};
-    tile_init(sm);
+__device__ __forceinline__ bool gstep_slot(const GArgs& g, uint32_t slot, uint32_t bits, const TileSmem& sm, uint64_t* sc,
+                                           uint32_t& par) {
     const SlotArgs& a = g.a;
     const int m = g.m, n = 1 << m;
-    const uint32_t slot = first + blockIdx.x;
     uint32_t* x = a.x + (size_t)slot * n;
     uint32_t* tl = a.tbuf + (size_t)slot * 2 * n;
     const F2* cc2 = a.c2 + (size_t)slot * 2 * n;
@@ -476,7 +473,6 @@ __global__ void __launch_bounds__(NT, 2) gstep_kernel(GArgs g, uint32_t first, u
     uint32_t pos = a.pos[slot];
     const F2K* tt2 = a.tab2 + glt_tile_off(m);
     const F1* tt1 = a.tab1 + glt_tile_off(m);
-    uint32_t par = 0;
     int st = kStepOk;
     bool carry_ok = true;
     for (uint32_t it = 0; it < bits && pos < nb; ++it, ++pos) {
@@ -491,11 +487,25 @@ __global__ void __launch_bounds__(NT, 2) gstep_kernel(GArgs g, uint32_t first, u
         if (st == kStepTimeout) break;
         carry_ok &= st == kStepOk;
     }
+    __syncthreads();   // every thread has read pos before it is written
     if (threadIdx.x == 0) {
         a.pos[slot] = pos;
         if (st == kStepTimeout) a.err[slot] = kErrTimeout;
         else if (!carry_ok) a.err[slot] = 1;
     }
+    return st != kStepTimeout;
+}
+
+// The uniform launch, global mode: one block per slot first + blockIdx.x.
+template <int NT>
+__global__ void __launch_bounds__(NT, 2) gstep_kernel(GArgs g, uint32_t first, uint32_t bits) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ uint64_t sc[CarryScratch<NT>::words];
+    __shared__ uint64_t bars[2];
+    const TileSmem sm{smem_raw, bars};
+    tile_init(sm);
+    uint32_t par = 0;
+    gstep_slot<NT>(g, first + blockIdx.x, bits, sm, sc, par);
 }
 
 // x[out] <- x[ia] x[ib] R^-1, global mode; spec: n-element scratch for F(x[ib]).
@@ -535,14 +545,15 @@ __global__ void __launch_bounds__(NT, 2) gmul_kernel(GArgs g, uint32_t out, uint
 // tile DIF, then the wraparound factors from the half transform of N.
 template <int NT>
 __global__ void __launch_bounds__(NT, 2) gsetup_kernel(GArgs g, const uint32_t* nl, const uint32_t* npl, F2* c2, F1* c1,
-                                                       F2 inv8h2, F1 inv8h1, uint32_t first) {
+                                                       F2 inv8h2, F1 inv8h1, uint32_t first, const uint32_t* slots) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ uint64_t bars[2];
     const TileSmem sm{smem_raw, bars};
     tile_init(sm);
     const SlotArgs& a = g.a;
     const int m = g.m, n = 1 << m, h = n / 2;
-    const uint32_t slot = first + blockIdx.x;
+    const uint32_t slot = slots ? slots[blockIdx.x] : first + blockIdx.x;
+    const size_t row = slots ? blockIdx.x : slot;
     F2* w2 = g.w2 + (size_t)slot * n;
     F1* w1 = g.w1 + (size_t)slot * n;
     F2* o2 = c2 + (size_t)slot * 2 * n;
@@ -551,10 +562,10 @@ __global__ void __launch_bounds__(NT, 2) gsetup_kernel(GArgs g, const uint32_t* 
     const F1* tt1 = a.tab1 + glt_tile_off(m);
     uint32_t par = 0;
     bool ok = false;
-    g_fwd<NT>(m, true, npl + (size_t)slot * n, w2, w1, a.tab2, a.tab1);
+    g_fwd<NT>(m, true, npl + row * n, w2, w1, a.tab2, a.tab1);
     if (tile_phase<NT>(w2, w1, n, tt2, tt1, SpecStoreRT{o2, o1, n / 8}, kTileDifOp, sm, par)) {
         par = tile_par_next(par, n);
-        pack_pairs(nl + (size_t)slot * n, w2, w1, h, NT);
+        pack_pairs(nl + row * n, w2, w1, h, NT);
         const F2K* ht2 = a.tab2 + glt_half_off(m);
         const F1* ht1 = a.tab1 + glt_half_off(m);
         if (m - 1 > kTileLog) g_fwd<NT>(m - 1, false, nullptr, w2, w1, ht2, ht1);

@@ -184,15 +184,14 @@ __device__ __noinline__ bool redc_wrap(F2* s2, F1* s1, const uint32_t* tl, uint3
     return wrap_combine<M, NT>(s2, s1, tl, x, sc);
 }
 
-// Up to `bits` steps x <- x^2 c^bit R^-1 on slot first + blockIdx.x (cpu.rs:543-556).
+// Up to `bits` steps x <- x^2 c^bit R^-1 on one slot (cpu.rs:543-556), the whole block, the
+// vector in `smem_raw` (24 n bytes). Used by the uniform launch and the mixed-length launch.
 template <int M, int NT>
-__global__ void __launch_bounds__(NT, (M <= 12 ? 2 : 1)) step_kernel(SlotArgs a, uint32_t first, uint32_t bits) {
+__device__ __forceinline__ void step_slot(const SlotArgs& a, uint32_t slot, uint32_t bits, unsigned char* smem_raw,
+                                          uint64_t* sc) {
     constexpr int N = 1 << M;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
     F2* s2 = reinterpret_cast<F2*>(smem_raw);
     F1* s1 = reinterpret_cast<F1*>(smem_raw + 16 * N);
-    __shared__ uint64_t sc[CarryScratch<NT>::words];
-    const uint32_t slot = first + blockIdx.x;
     uint32_t* x = a.x + (size_t)slot * N;
     uint32_t* tl = a.tbuf + (size_t)slot * 2 * N;
     const F2* cc2 = a.c2 + (size_t)slot * 2 * N;
@@ -210,10 +209,19 @@ __global__ void __launch_bounds__(NT, (M <= 12 ? 2 : 1)) step_kernel(SlotArgs a,
         ok &= carry_product<M, NT>(s2, s1, tl, sc) == 0;
         ok &= redc_wrap<M, NT>(s2, s1, tl, x, cc2, cc1, a.tab2, a.tab1, sc);
     }
+    __syncthreads();   // every thread has read pos before it is written
     if (threadIdx.x == 0) {
         a.pos[slot] = pos;
         if (!ok) a.err[slot] = 1;
     }
+}
+
+// The uniform launch: one block per slot first + blockIdx.x.
+template <int M, int NT>
+__global__ void __launch_bounds__(NT, (M <= 12 ? 2 : 1)) step_kernel(SlotArgs a, uint32_t first, uint32_t bits) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ uint64_t sc[CarryScratch<NT>::words];
+    step_slot<M, NT>(a, first + blockIdx.x, bits, smem_raw, sc);
 }
 
 // x[out] <- x[ia] x[ib] R^-1 with slot out's modulus (cpu.rs:558-571), one block. spec: n
@@ -240,20 +248,24 @@ __global__ void __launch_bounds__(NT) mul_kernel(SlotArgs a, uint32_t out, uint3
     if (threadIdx.x == 0 && !ok) a.err[out] = 1;
 }
 
-// Per-slot constants of slot first + blockIdx.x from its N and N' limbs (k = n each):
+// Per-slot constants of slot first + blockIdx.x (or slots[blockIdx.x]) from its N and N' limbs
+// (k = n each):
 // F(N') in fused-pass order (cpu.rs:518), then the wraparound factors A | B from the half
 // transform of N (cpu.rs:239-284; computed on the host by the reference's GPU backend).
 // inv8h = (8 h)^-1 in each field.
 template <int M, int NT>
 __global__ void __launch_bounds__(NT) setup_kernel(const uint32_t* nl, const uint32_t* npl, F2* c2, F1* c1, const F2K* tab2,
-                                                   const F1* tab1, F2 inv8h2, F1 inv8h1, uint32_t first) {
+                                                   const F1* tab1, F2 inv8h2, F1 inv8h1, uint32_t first,
+                                                   const uint32_t* slots) {
     constexpr int N = 1 << M, H = N / 2;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     F2* s2 = reinterpret_cast<F2*>(smem_raw);
     F1* s1 = reinterpret_cast<F1*>(smem_raw + 16 * N);
-    const uint32_t slot = first + blockIdx.x;
-    const uint32_t* np = npl + (size_t)slot * N;
-    const uint32_t* nn = nl + (size_t)slot * N;
+    // Rows of nl / npl: all slots from `first` on, or (with a slot list) one row per listed slot.
+    const uint32_t slot = slots ? slots[blockIdx.x] : first + blockIdx.x;
+    const size_t row = slots ? blockIdx.x : slot;
+    const uint32_t* np = npl + row * N;
+    const uint32_t* nn = nl + row * N;
     F2* o2 = c2 + (size_t)slot * 2 * N;
     F1* o1 = c1 + (size_t)slot * 2 * N;
     fwd_limbs<M, NT>(np, N, s2, s1, tab2, tab1);

@@ -1,0 +1,344 @@
+"""Served Fermat stream: continuous batching of PRP tests and mul requests of different sizes
+(no counterpart in the reference, whose backend runs one uniform batch at a time).
+
+Requests arrive as a Poisson process. Each transform length has a lane: uniform batches
+("segments") whose slots keep their Montgomery state and exponent on the device. A request is
+admitted as soon as a slot of its length is free; a lane grows by one segment while the device
+memory budget allows (admission by the per-slot bytes of its length), else the request waits.
+Every tick runs `quantum` steps on every busy slot of every lane in one mixed-length plan launch
+(persistent blocks over a device work queue, replayed from a CUDA graph), then reads back the
+slots that finished and refills them in place with waiting requests: the batch is never drained.
+
+A Fermat request loads 1, sets the exponent N - 1 and reports the verdict x == 1; a mul request
+(a b mod N) takes two slots of the same modulus and one mul launch. Each request's time to
+verdict runs from its arrival to the tick that read its result.
+
+    python -m montmul_b200 serve [--load 0.7 0.95] [--requests 150] [--lo 10000] [--hi 200000]
+"""
+from __future__ import annotations
+
+import math
+import statistics
+import time
+from collections import deque
+from concurrent.futures import ThreadPoolExecutor
+from dataclasses import dataclass, field
+from typing import Optional
+
+from . import gmp
+from .batch import ModBatch, MontMulError, Params
+
+MAX_DRAW = 1 << 30
+# Exponents p of Mersenne primes 2^p - 1 (Lucas-Lehmer; the published list), used as the prime
+# requests of the stream: a seeded next_prime search at these sizes takes far longer than the run.
+MERSENNE_P = (4253, 4423, 9689, 9941, 11213, 19937, 21701, 23209, 44497, 86243, 110503, 132049, 216091)
+
+
+@dataclass
+class Request:
+    rid: int
+    kind: str             # "fermat" or "mul"
+    n: int
+    arrival: float        # seconds after the start of the run
+    a: int = 0
+    b: int = 0
+    prime: bool = False   # drawn as a known prime
+    length: int = 0
+    admitted: Optional[float] = None
+    done: Optional[float] = None
+    verdict: Optional[bool] = None
+    value: Optional[int] = None
+    raw: Optional[int] = None
+
+
+def stream(count: int, rate: float, lo: int, hi: int, prime_frac: float = 0.1, mul_frac: float = 0.05,
+           seed: int = 2026):
+    """`count` requests with exponential inter-arrival times of mean 1/rate: bit sizes log-uniform
+    in [lo, hi]; a `prime_frac` share are Mersenne primes in range, a `mul_frac` share mul
+    requests, the rest random odd N with the top bit set (composite but for a vanishing share)."""
+    rng = gmp.RandState(seed)
+    primes = [p for p in MERSENNE_P if lo <= p <= hi]
+    out, t = [], 0.0
+    for rid in range(count):
+        u = (rng.random_below(MAX_DRAW - 1) + 1) / MAX_DRAW
+        t += -math.log(u) / rate
+        v = rng.random_below(MAX_DRAW) / MAX_DRAW
+        bits = int(round(math.exp(math.log(lo) + v * (math.log(hi) - math.log(lo)))))
+        kind_draw = rng.random_below(1000) / 1000.0
+        if kind_draw < mul_frac:
+            n = rng.random_bits(bits) | (1 << (bits - 1)) | 1
+            out.append(Request(rid, "mul", n, t, a=rng.random_below(n), b=rng.random_below(n)))
+        elif kind_draw < mul_frac + prime_frac and primes:
+            p = primes[rng.random_below(len(primes))]
+            out.append(Request(rid, "fermat", (1 << p) - 1, t, prime=True))
+        else:
+            n = rng.random_bits(bits) | (1 << (bits - 1)) | 1
+            out.append(Request(rid, "fermat", n, t))
+    return out
+
+
+def per_slot_bytes(lib, length: int) -> int:
+    return int(lib.mm_b200_batch_bytes(2, length, length // 64 + 1) - lib.mm_b200_batch_bytes(1, length, length // 64 + 1))
+
+
+@dataclass
+class Segment:
+    batch: ModBatch
+    free: list
+    active: dict = field(default_factory=dict)   # slot -> Request
+
+
+class Server:
+    """Lanes of segments per transform length, one plan over every segment."""
+
+    def __init__(self, dev, base: int = 3, quantum: int = 128, segment_slots: int = 0, budget_frac: float = 0.5,
+                 tuned: bool = True):
+        from .backend import lib
+        self.dev = dev
+        self.lib = lib()
+        self.base = base
+        self.quantum = quantum
+        self.lengths = dev.supported_lengths()
+        self.segment_slots = segment_slots or 2 * 2 * dev.sm_count()
+        self.budget = int(budget_frac * dev.free_memory())
+        self.used = 0
+        self.lanes = {}           # length -> [Segment]
+        self.plan = None
+        self.plan_dirty = False
+        self.tuned = tuned
+        self.steps_done = 0
+        self.ticks = []           # (t, busy slots, slot-steps run)
+
+    # ---- admission ----
+    def _grow(self, length: int) -> Optional[Segment]:
+        k = length // 2
+        slots = self.segment_slots
+        need = slots * per_slot_bytes(self.lib, length)
+        if self.used + need > self.budget:
+            slots = (self.budget - self.used) // per_slot_bytes(self.lib, length)
+            if slots < 1:
+                return None
+            need = slots * per_slot_bytes(self.lib, length)
+        bits = 32 * k - 4
+        dummy = (1 << (bits - 1)) | 1
+        b = ModBatch(self.dev, [dummy] * slots, self.base)
+        b.set_exponents([0] * slots)
+        if self.tuned:
+            from . import tune
+            tune.apply(b)
+        seg = Segment(b, list(range(slots - 1, -1, -1)))
+        self.lanes.setdefault(length, []).append(seg)
+        self.used += need
+        self.plan_dirty = True
+        return seg
+
+    def _slots_for(self, length: int, count: int):
+        """`count` free slots of one segment of the lane, growing the lane if needed."""
+        for seg in self.lanes.get(length, []):
+            if len(seg.free) >= count:
+                return seg, [seg.free.pop() for _ in range(count)]
+        seg = self._grow(length)
+        if seg is None or len(seg.free) < count:
+            return None, None
+        return seg, [seg.free.pop() for _ in range(count)]
+
+    def admit(self, waiting: deque, now: float) -> None:
+        """Admits waiting requests in arrival order while slots are free (a request that does not
+        fit stays; later ones of other lengths may still pass it)."""
+        fermat = {}   # segment id -> (segment, slots, requests)
+        kept = deque()
+        while waiting:
+            r = waiting.popleft()
+            if not r.length:
+                r.length = Params.for_bits(r.n.bit_length(), self.lengths).len
+            need = 2 if r.kind == "mul" else 1
+            seg, slots = self._slots_for(r.length, need)
+            if seg is None:
+                kept.append(r)
+                continue
+            r.admitted = now
+            if r.kind == "mul":
+                self._mul(seg, slots, r)
+                continue
+            e = fermat.setdefault(id(seg), (seg, [], []))
+            e[1].append(slots[0])
+            e[2].append(r)
+        waiting.extend(kept)
+        for seg, slots, reqs in fermat.values():
+            seg.batch.refill(slots, [r.n for r in reqs], [1] * len(reqs), [r.n - 1 for r in reqs])
+            for s, r in zip(slots, reqs):
+                seg.active[s] = r
+
+    def _mul(self, seg: Segment, slots, r: Request) -> None:
+        b = seg.batch
+        b.refill(slots, [r.n, r.n], [r.a, r.b], [0, 0])
+        b.mul(slots[0], slots[0], slots[1])
+        m = b.moduli[slots[0]]
+        r.value = gmp.mulmod(b.read_raw_slots(slots[:1])[0], m.rinv, m.n)
+        r.done = time.perf_counter() - self.t0
+        seg.free.extend(slots)
+
+    # ---- ticks ----
+    def _plan(self):
+        from .backend import Plan
+        if self.plan is None or self.plan_dirty:
+            if self.plan is not None:
+                self.plan.close()
+            segs = [s.batch for segs in self.lanes.values() for s in segs]
+            self.plan = Plan(segs, self.quantum)
+            self.plan_dirty = False
+        return self.plan
+
+    def busy(self) -> int:
+        return sum(len(s.active) for segs in self.lanes.values() for s in segs)
+
+    def tick(self) -> int:
+        """One quantum on every busy slot, then the finished slots are read and freed."""
+        plan = self._plan()
+        run = 0
+        for segs in self.lanes.values():
+            for seg in segs:
+                for s in seg.active:
+                    run += min(self.quantum, seg.batch.remaining(s))
+        plan.run(self.quantum)
+        now = time.perf_counter() - self.t0
+        self.steps_done += run
+        self.ticks.append((now, self.busy(), run))
+        finished = 0
+        for segs in self.lanes.values():
+            for seg in segs:
+                done = [s for s in seg.active if seg.batch.remaining(s) == 0]
+                if not done:
+                    continue
+                raws = seg.batch.read_raw_slots(done)
+                for s, raw in zip(done, raws):
+                    r = seg.active.pop(s)
+                    m = seg.batch.moduli[s]
+                    r.raw = raw
+                    r.verdict = raw == m.r or raw == m.r + m.n
+                    r.done = now
+                    seg.free.append(s)
+                    finished += 1
+        return finished
+
+    def serve(self, reqs):
+        """Runs the whole stream in real time; returns the requests with their results."""
+        pending = deque(sorted(reqs, key=lambda r: r.arrival))
+        waiting = deque()
+        self.t0 = time.perf_counter()
+        left = len(reqs)
+        while left:
+            now = time.perf_counter() - self.t0
+            while pending and pending[0].arrival <= now:
+                waiting.append(pending.popleft())
+            before = sum(1 for r in reqs if r.done is not None)
+            if waiting:
+                self.admit(waiting, now)
+            if self.busy():
+                self.tick()
+            elif pending and not waiting:
+                time.sleep(max(0.0, min(0.05, pending[0].arrival - (time.perf_counter() - self.t0))))
+            elif waiting and not self.busy():
+                raise MontMulError("a request fits no lane within the memory budget")
+            left -= sum(1 for r in reqs if r.done is not None) - before
+        return reqs
+
+    def close(self):
+        if self.plan is not None:
+            self.plan.close()
+            self.plan = None
+
+
+def capacity(reqs, step_s) -> float:
+    """Fermat tests per second the GPU completes at full occupancy for this request mix:
+    1 / the mean of (exponent bits x seconds per slot-step at the request's length)."""
+    work = [r.n.bit_length() * step_s(Params.for_bits(r.n.bit_length(), _LENGTHS).len) for r in reqs
+            if r.kind == "fermat"]
+    return 1.0 / statistics.mean(work)
+
+
+_LENGTHS = [1 << e for e in range(3, 25)]
+
+
+def check(reqs, threads: int = 32) -> int:
+    """Every verdict against GMP's pow_mod(3, N - 1, N) == 1, every mul against a b mod N."""
+    def one(r):
+        if r.kind == "mul":
+            if r.value != r.a * r.b % r.n:
+                raise MontMulError(f"request {r.rid}: mul disagrees")
+        else:
+            want = gmp.powm(3, r.n - 1, r.n) == 1
+            if r.verdict != want or (r.prime and not r.verdict):
+                raise MontMulError(f"request {r.rid} ({r.n.bit_length()} bits): verdict {r.verdict}, pow_mod {want}")
+        return 1
+    with ThreadPoolExecutor(threads) as ex:
+        return sum(ex.map(one, reqs))
+
+
+def percentile(v, q: float) -> float:
+    s = sorted(v)
+    if not s:
+        return float("nan")
+    i = min(len(s) - 1, max(0, int(math.ceil(q * len(s))) - 1))
+    return s[i]
+
+
+def summarize(server: Server, reqs, uniform_modsq: float, rate: float, cap: float) -> dict:
+    ferm = [r for r in reqs if r.kind == "fermat"]
+    muls = [r for r in reqs if r.kind == "mul"]
+    lat = [r.done - r.arrival for r in ferm]
+    end = max(r.done for r in reqs)
+    steps = sum(r.n.bit_length() for r in ferm)
+    # Steady window: from the first completion to the last arrival, when the stream is neither
+    # filling nor draining.
+    t_a = min(r.done for r in ferm)
+    t_b = max(r.arrival for r in reqs)
+    win = [(t, run) for t, _, run in server.ticks if t_a <= t <= t_b]
+    win_modsq = (sum(run for _, run in win) / (win[-1][0] - win[0][0])) if len(win) > 2 else None
+    return {
+        "offered_tests_per_s": rate, "capacity_tests_per_s": cap, "load": rate / cap,
+        "requests": len(reqs), "fermat": len(ferm), "mul": len(muls),
+        "primes": sum(1 for r in ferm if r.prime), "prp": sum(1 for r in ferm if r.verdict),
+        "seconds": end, "tests_per_hour": 3600.0 * len(ferm) / end,
+        "modsq_per_s": steps / end, "steady_modsq_per_s": win_modsq,
+        "uniform_modsq_per_s": uniform_modsq,
+        "steady_over_uniform": (win_modsq / uniform_modsq) if win_modsq else None,
+        "p50_s": percentile(lat, 0.5), "p99_s": percentile(lat, 0.99),
+        "mul_p50_s": percentile([r.done - r.arrival for r in muls], 0.5) if muls else None,
+        "ticks": len(server.ticks), "quantum": server.quantum,
+        "lanes": {str(L): sum(len(s.batch.moduli) for s in segs) for L, segs in server.lanes.items()},
+        "device_bytes": server.used,
+    }
+
+
+def main(args) -> dict:
+    from .backend import B200
+    from . import tune
+    dev = B200(device=args.device)
+    # Seconds per slot-step at full occupancy per length (the tuned table, measured if absent).
+    per = tune.tune(dev, sorted({Params.for_bits(b, dev.supported_lengths()).len
+                                 for b in (args.lo, args.hi)} | {1 << e for e in range(10, 15)}), log=lambda *_: None)
+
+    def step_s(length):
+        return per[str(length)]["step_ns"] * 1e-9
+
+    probe = stream(args.requests, 1.0, args.lo, args.hi, seed=args.seed)
+    cap = capacity(probe, step_s)
+    # The plain uniform-batch rate of the same mix: total steps over their uniform-batch time.
+    ferm = [r for r in probe if r.kind == "fermat"]
+    uniform = sum(r.n.bit_length() for r in ferm) / sum(
+        r.n.bit_length() * step_s(Params.for_bits(r.n.bit_length(), dev.supported_lengths()).len) for r in ferm)
+    results = []
+    for load in args.load:
+        rate = load * cap
+        reqs = stream(args.requests, rate, args.lo, args.hi, seed=args.seed)
+        srv = Server(dev, quantum=args.quantum)
+        srv.serve(reqs)
+        srv.close()
+        checked = check(reqs) if not args.no_check else 0
+        s = summarize(srv, reqs, uniform, rate, cap)
+        s["checked"] = checked
+        results.append(s)
+    return {"workload": f"{args.requests} requests, bits log-uniform in [{args.lo}, {args.hi}], "
+                        f"10% Mersenne primes, 5% mul, Poisson arrivals (seed {args.seed})",
+            "loads": results}

@@ -1,0 +1,188 @@
+"""Autotuner and cached per-length schedule table (no counterpart in the reference, whose planner
+fixes the schedule: montmul/src/gpu/plan.rs:26-60).
+
+For each transform length L the tuner times every schedule the library can switch at run time on
+the device and keeps the fastest:
+
+  - shared vs global mode: L <= 4096 shared only, L = 8192 and 16384 both (16384 in shared mode
+    holds one block per SM, in global mode two), L >= 32768 global only;
+  - steps per launch (launch_steps): a longer launch saves launch gaps, a shorter one bounds how
+    long a batch holds the GPU.
+
+It records the winner's time per slot-step (step_ns), which also orders the work items of a
+mixed-length launch. The fixed parts of a schedule are reported beside it: threads per block,
+the radix schedule of the length-n transform, the tile length of global mode and the blocks per
+SM. The table is JSON keyed by device name, cached at $MONTMUL_B200_SCHEDULES or
+~/.cache/montmul_b200/schedules.json:
+
+    python -m montmul_b200.tune [--lengths 8192 16384 ...] [--force]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import sys
+import time
+
+TILE = 2048           # global mode's tile length (elements of n)
+MAX_SHARED_N = 8192   # n <= 8192 fits the shared-memory kernels
+MIN_GLOBAL_N = 4096   # global mode from n = 4096 (L = 8192)
+LAUNCH_STEPS = (64, 512)
+
+
+def cache_path() -> str:
+    p = os.environ.get("MONTMUL_B200_SCHEDULES")
+    if p:
+        return p
+    return os.path.join(os.path.expanduser("~"), ".cache", "montmul_b200", "schedules.json")
+
+
+def radix_schedule(m: int):
+    """Radix of every pass of a length-2^m transform (the device schedule, mm_common.h)."""
+    if m <= 3:
+        return [{1: 2, 2: 4, 3: 8}[m]] if m >= 1 else []
+    if m % 3 == 0:
+        return [8] * (m // 3)
+    if m % 3 == 1:
+        return [4, 4] + [8] * (m // 3 - 1)
+    return [4] + [8] * (m // 3)
+
+
+def threads_for(m: int) -> int:
+    """Threads per block of the shared-memory kernels (mm_abi.h threads_for)."""
+    return 32 if m - 3 <= 5 else (256 if m - 3 >= 8 else 1 << (m - 3))
+
+
+def fixed_parts(length: int, global_mode: bool):
+    n = length // 2
+    m = n.bit_length() - 1
+    if global_mode:
+        g = m - TILE.bit_length() + 1
+        return {"threads": 256, "blocks_per_sm": 2, "tile": TILE,
+                "radix": {"global": radix_schedule(g), "tile": radix_schedule(TILE.bit_length() - 1)}}
+    per_sm = 2 if m <= 12 else 1
+    return {"threads": threads_for(m), "blocks_per_sm": per_sm, "tile": None, "radix": radix_schedule(m)}
+
+
+def candidates(length: int):
+    n = length // 2
+    modes = []
+    if n <= MAX_SHARED_N:
+        modes.append(False)
+    if n >= MIN_GLOBAL_N:
+        modes.append(True)
+    return [(g, s) for g in modes for s in LAUNCH_STEPS]
+
+
+def bits_for(length: int) -> int:
+    """Top of the bucket: the largest modulus size with this length (k = L/2 limbs, batch.rs:20)."""
+    return 16 * length - 4
+
+
+def measure(dev, length: int, global_mode: bool, launch_steps: int, slots: int, steps: int, seed: int = 2026):
+    """Seconds per slot-step of one schedule on a synthetic batch (random odd moduli at the top of
+    the bucket, random exponents), after a warm-up launch."""
+    from .batch import ModBatch
+    from .gmp import RandState
+    rng = RandState(seed)
+    bits = bits_for(length)
+    moduli = [rng.random_bits(bits) | (1 << (bits - 1)) | 1 for _ in range(slots)]
+    exps = [rng.random_bits(steps + 8) | (1 << (steps + 7)) for _ in range(slots)]
+    b = ModBatch(dev, moduli, 3)
+    be, st = b.backend_and_state()
+    be.set_schedule(st, global_mode, launch_steps)
+    b.load_all([1] * slots)
+    b.set_exponents(exps)
+    b.run(8)
+    t = time.perf_counter()
+    b.run(steps)
+    dt = time.perf_counter() - t
+    return dt / (slots * steps)
+
+
+def tune_length(dev, length: int, budget_s: float = 4.0):
+    """The fastest schedule of one length, with every candidate's time."""
+    sms = dev.sm_count()
+    n = length // 2
+    # Enough slots for several waves of resident blocks, and enough steps for ~budget_s / candidates.
+    slots = sms * (8 if n <= 8192 else 4)
+    probe = measure(dev, length, candidates(length)[0][0], 512, slots, 4)
+    cands = candidates(length)
+    steps = max(8, min(2000, int(budget_s / len(cands) / (probe * slots))))
+    results = []
+    for g, s in cands:
+        sec = measure(dev, length, g, s, slots, steps)
+        results.append({"global": g, "launch_steps": s, "step_ns": sec * 1e9})
+    best = min(results, key=lambda r: r["step_ns"])
+    out = dict(best)
+    out.update(fixed_parts(length, best["global"]))
+    out["slots"] = slots
+    out["steps"] = steps
+    out["candidates"] = results
+    return out
+
+
+def load_table():
+    try:
+        with open(cache_path()) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+def save_table(table) -> None:
+    p = cache_path()
+    os.makedirs(os.path.dirname(p), exist_ok=True)
+    tmp = p + ".tmp"
+    with open(tmp, "w") as f:
+        json.dump(table, f, indent=1, sort_keys=True)
+    os.replace(tmp, p)
+
+
+def schedule_for(device_name: str, length: int, table=None):
+    """The cached schedule of one length on one device, or None."""
+    table = load_table() if table is None else table
+    return table.get(device_name, {}).get(str(length))
+
+
+def apply(batch, table=None) -> bool:
+    """Sets the cached schedule of the batch's length on its backend; False when none is cached."""
+    be, st = batch.backend_and_state()
+    sc = schedule_for(be.device_name(), batch.params.len, table)
+    if not sc:
+        return False
+    be.set_schedule(st, sc["global"], sc["launch_steps"], sc["step_ns"])
+    return True
+
+
+def tune(dev, lengths, force: bool = False, log=print):
+    table = load_table()
+    name = dev.device_name()
+    per = table.setdefault(name, {})
+    for length in lengths:
+        if str(length) in per and not force:
+            continue
+        r = tune_length(dev, length)
+        per[str(length)] = r
+        log(f"L={length}: {'global' if r['global'] else 'shared'} launch_steps={r['launch_steps']} "
+            f"{r['step_ns'] / 1e3:.2f} us/slot-step")
+        save_table(table)
+    return per
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--lengths", type=int, nargs="*", default=[1 << e for e in range(8, 18)])
+    ap.add_argument("--force", action="store_true", help="re-measure lengths already in the table")
+    ap.add_argument("--device", type=int, default=0)
+    a = ap.parse_args(argv)
+    from .backend import B200
+    dev = B200(device=a.device)
+    per = tune(dev, a.lengths, a.force)
+    print(json.dumps({str(k): {kk: v for kk, v in per[str(k)].items() if kk != "candidates"} for k in a.lengths}))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,51 @@
+"""The continuous-batching serve loop: requests of several sizes admitted while others run, slots
+refilled in place. Each Fermat result must be the same raw Montgomery value as the same request
+run alone in its own batch, each verdict equal to pow_mod's, each mul equal to a b mod N."""
+import pytest
+
+from montmul_b200 import ModBatch, fermat
+from montmul_b200.gmp import powm
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def dev():
+    from montmul_b200 import B200
+    return B200()
+
+
+def _alone_raw(dev, n):
+    b = ModBatch(dev, [n], 3)
+    b.load_all([1])
+    b.set_exponents([n - 1])
+    while b.remaining(0):
+        b.run(1 << 16)
+    return b.read_raw(0)
+
+
+def test_served_stream_same_as_alone(dev):
+    from montmul_b200 import serve
+    reqs = serve.stream(40, 400.0, 2000, 40_000, prime_frac=0.2, mul_frac=0.1, seed=17)
+    # Small segments force several segments per lane and waiting requests.
+    srv = serve.Server(dev, quantum=64, segment_slots=6, tuned=False)
+    srv.serve(reqs)
+    srv.close()
+    assert all(r.done is not None for r in reqs)
+    assert len(srv.ticks) > 3 and max(b for _, b, _ in srv.ticks) > 1
+    assert len(srv.lanes) >= 3
+    for r in reqs:
+        if r.kind == "mul":
+            assert r.value == r.a * r.b % r.n
+            continue
+        assert r.verdict == (powm(3, r.n - 1, r.n) == 1)
+        if r.prime:
+            assert r.verdict
+        assert r.raw == _alone_raw(dev, r.n), f"request {r.rid} ({r.n.bit_length()} bits)"
+    assert serve.check(reqs) == len(reqs)
+
+
+def test_fermat_driver_on_mersenne_primes(dev):
+    """fermat() (batch.rs:187-198) on known primes of two lengths and a composite neighbour."""
+    assert fermat(dev, [(1 << 4423) - 1], 3) == [True]
+    assert fermat(dev, [(1 << 9689) - 1, (1 << 9689) + 1], 3) == [True, False]

@@ -1,0 +1,79 @@
+"""Host-side logic of the tools around the kernels, without a GPU: the autotuner's fixed schedule
+facts, the mixed and served workloads, the CLI's sequence and percentile helpers."""
+import math
+
+from montmul_b200 import mixed, serve, tune
+from montmul_b200.__main__ import tribonacci
+from montmul_b200.batch import Params
+
+LENGTHS = [1 << e for e in range(3, 25)]
+
+
+def test_radix_schedule_covers_every_stage():
+    for m in range(1, 24):
+        sched = tune.radix_schedule(m)
+        assert sum(int(math.log2(r)) for r in sched) == m
+        assert all(r in (2, 4, 8) for r in sched)
+        if m >= 5 or m == 3:
+            assert sched[-1] == 8   # the fused last pass is radix 8 (m = 4 runs [4, 4])
+
+
+def test_tune_candidates_by_length():
+    assert tune.candidates(4096) == [(False, s) for s in tune.LAUNCH_STEPS]
+    assert {g for g, _ in tune.candidates(8192)} == {False, True}
+    assert {g for g, _ in tune.candidates(16384)} == {False, True}
+    assert {g for g, _ in tune.candidates(32768)} == {True}
+    assert tune.fixed_parts(1 << 20, True)["radix"]["global"] == tune.radix_schedule(19 - 11)
+
+
+def test_tune_table_roundtrip(tmp_path, monkeypatch):
+    monkeypatch.setenv("MONTMUL_B200_SCHEDULES", str(tmp_path / "s.json"))
+    tune.save_table({"dev": {"8192": {"global": False, "launch_steps": 512, "step_ns": 680.0}}})
+    assert tune.schedule_for("dev", 8192)["step_ns"] == 680.0
+    assert tune.schedule_for("dev", 4096) is None
+    assert tune.schedule_for("other", 8192) is None
+
+
+def test_mixed_workload():
+    w = mixed.workload(500, 8192, 300_000, 1000, 7)
+    assert w == mixed.workload(500, 8192, 300_000, 1000, 7)
+    for bits, n, c, e in w:
+        assert 8192 <= bits <= 300_000 and n.bit_length() == bits and n % 2 == 1
+        assert c in (2, 3, 4) and e == (n - 1) >> (bits - 1000) and e.bit_length() == 1000
+    # log-uniform: about half the slots below the geometric midpoint
+    mid = math.sqrt(8192 * 300_000)
+    below = sum(1 for bits, *_ in w if bits < mid)
+    assert 200 < below < 300
+    assert {Params.for_bits(b, LENGTHS).len for b, *_ in w} == {1024, 2048, 4096, 8192, 16384, 32768}
+
+
+def test_serve_stream():
+    r = serve.stream(400, 10.0, 10_000, 200_000, seed=3)
+    assert r == serve.stream(400, 10.0, 10_000, 200_000, seed=3)
+    assert all(b.arrival > a.arrival for a, b in zip(r, r[1:]))
+    gaps = [b.arrival - a.arrival for a, b in zip(r, r[1:])]
+    assert 0.07 < sum(gaps) / len(gaps) < 0.13   # mean 1 / rate
+    kinds = [x.kind for x in r]
+    assert 5 <= kinds.count("mul") <= 40
+    primes = [x for x in r if x.prime]
+    assert 20 <= len(primes) <= 70
+    for x in primes:
+        assert x.n + 1 == 1 << x.n.bit_length() and x.n.bit_length() in serve.MERSENNE_P
+    for x in r:
+        assert x.n % 2 == 1
+        if x.kind == "mul":
+            assert 0 <= x.a < x.n and 0 <= x.b < x.n
+
+
+def test_capacity_and_percentile():
+    reqs = [serve.Request(0, "fermat", (1 << 9999) | 1, 0.0), serve.Request(1, "fermat", (1 << 19999) | 1, 0.0),
+            serve.Request(2, "mul", 7, 0.0)]
+    cap = serve.capacity(reqs, lambda length: 1e-6 * length / 1024)
+    work = [10_000 * 1e-6 * 1024 / 1024, 20_000 * 1e-6 * 2048 / 1024]
+    assert abs(cap - 1 / (sum(work) / 2)) < 1e-9
+    assert serve.percentile([3, 1, 2, 4], 0.5) == 2
+    assert serve.percentile(list(range(1, 101)), 0.99) == 99
+
+
+def test_tribonacci_matches_the_reference_sequence():
+    assert [tribonacci(i) for i in range(10)] == [0, 0, 1, 1, 2, 4, 7, 13, 24, 44]
