@@ -40,6 +40,11 @@ def g_of_n(n: int) -> int:
     return 2 * n * lg + (n // 2) * (lg - 1) + 7 * n
 
 
+# dram__bytes_read.sum + dram__bytes_write.sum of one step_kernel launch at L = 8,192 (1,184
+# slots x 16 steps): 360.3 MB + 95.6 MB, per slot-step.
+DRAM_BYTES_PER_SLOT_STEP = (360.3e6 + 95.6e6) / (1184 * 16)
+
+
 def hbm_bytes_per_slot_step(n: int) -> int:
     """Per-slot constants that stream per step: F(N') and the A|B factors, 2n elements of 24 B."""
     return 48 * n
@@ -323,8 +328,15 @@ def main(argv=None):
     peaks = measured_peaks()
     hbm = peaks.get("hbm_gbs")
     achieved_gbs = slots * EBITS * hbm_bytes_per_slot_step(n) / per_step_s / 1e9
+    # DRAM traffic of one step-kernel launch: bytes per slot-step from the committed ncu capture
+    # of this kernel on this workload, times the slot-steps of one launch here.
+    steps_per_launch = EBITS * args.steps / max(1, launches)
+    traffic = DRAM_BYTES_PER_SLOT_STEP * slots * steps_per_launch
     roofline = {"bound": "int", "achieved": achieved_pairs / 1e9, "peak": peak_pairs / 1e9, "unit": "Gbfly/s",
-                "frac": achieved_pairs / peak_pairs, "traffic": None,
+                "frac": achieved_pairs / peak_pairs, "traffic": traffic,
+                "traffic_note": "bytes per launch: %.0f B per slot-step (dram__bytes_read+write of one ncu capture, "
+                                "profiles/step_kernel_score_L8192.md) x %d slots x %.0f steps per launch"
+                                % (DRAM_BYTES_PER_SLOT_STEP, slots, steps_per_launch),
                 "note": "butterfly pairs (GF(p^2) product + add + sub in both fields), G(n)=%d per modsq at "
                         "L=8192; peak = the kernels' own arithmetic in register-resident chains on all SMs, "
                         "measured in this run" % g_of_n(n)}

@@ -87,6 +87,10 @@ int mm_b200_set_exponent(mm_b200_batch *b, size_t i, const uint32_t *words, size
 int mm_b200_set_exponents(mm_b200_batch *b, const uint32_t *words, size_t ew, const uint32_t *nbits);
 /* Backend::run (transform.rs:69-70): up to `bits` steps on every slot with bits left. */
 int mm_b200_run(mm_b200_batch *b, size_t bits);
+/* Gpu::run_bare (gpu/mod.rs:109-111): like run, but each step stops after the squaring
+ * T = c x^2 and leaves x unchanged; it times the squaring alone for the overhead ratio
+ * (score.rs:140-159). Positions advance as in run. */
+int mm_b200_run_bare(mm_b200_batch *b, size_t bits);
 /* Backend::mul (transform.rs:71-72): slot out <- a b R^-1, slots sharing a modulus. */
 int mm_b200_mul(mm_b200_batch *b, size_t out, size_t a, size_t bb);
 /* Backend::read (transform.rs:73-74): k limbs in [0, 2N). */
@@ -123,6 +127,29 @@ uint64_t mm_b200_launches(const mm_b200_batch *b);
  * be serialized by the caller. */
 int mm_b200_mul_noalloc(const mm_b200_batch *b, size_t slot, const uint32_t *d_a, const uint32_t *d_b,
                         uint32_t *d_out, uint32_t *d_err, void *stream);
+
+/* ---- The Transform trait (transform.rs:22-46; the Gpu backend's impl, gpu/mod.rs:286-319) ----
+ * A buffer holds `count` vectors of length len = L, each L/2 elements of GF(M31^2) x GF(M61^2):
+ * coefficient j in the real part of element j, coefficient j + L/2 in the imaginary part.
+ * t_upload copies coefficients in (upload); t_download_raw writes the elements as
+ * count x L/2 x (re, im) field values in the reference's element order (download_raw; the CRT
+ * to exact coefficients, download, is host arithmetic on these). t_forward weights by zeta^j and
+ * runs the DIF (natural in, bit-reversed out); t_inverse runs the DIT and unweights by
+ * zeta^-j / n; t_pointwise sets out = scale a b per element, scales[v] for vector v (NULL: 1).
+ * t_load_forward uploads k limbs per vector, zero-padded to len, and forward-transforms them
+ * (load_forward). Results are canonical field values, bit-identical to the reference's Cpu. */
+typedef struct mm_b200_tbuf mm_b200_tbuf;
+int mm_b200_t_upload(mm_b200_device *dev, const uint32_t *coeffs, size_t len, size_t count, mm_b200_tbuf **out);
+int mm_b200_t_download_raw(const mm_b200_tbuf *b, uint32_t *f1, uint64_t *f2);
+int mm_b200_t_forward(mm_b200_tbuf *b, size_t len, size_t count);
+int mm_b200_t_inverse(mm_b200_tbuf *b, size_t len, size_t count);
+int mm_b200_t_pointwise(mm_b200_tbuf *out, const mm_b200_tbuf *a, const mm_b200_tbuf *b, const uint32_t *scales,
+                        size_t len, size_t count);
+int mm_b200_t_load_forward(mm_b200_device *dev, const uint32_t *limbs, size_t k, size_t len, size_t count,
+                           mm_b200_tbuf **out);
+size_t mm_b200_t_count(const mm_b200_tbuf *b);
+size_t mm_b200_t_len(const mm_b200_tbuf *b);
+void mm_b200_t_free(mm_b200_tbuf *b);
 
 /* ---- Schedules (no counterpart in the reference, whose planner fixes them: gpu/plan.rs:26-60) ----
  * global: 1 runs the batch in global mode (L >= 8192), 0 with the whole vector in shared memory
@@ -164,6 +191,11 @@ int mm_b200_plan_create(mm_b200_batch *const *batches, size_t count, size_t quan
 int mm_b200_plan_run_async(mm_b200_plan *p, size_t bits);
 int mm_b200_plan_sync(mm_b200_plan *p);
 int mm_b200_plan_run(mm_b200_plan *p, size_t bits);
+/* One launch in which the slots of batch i (in creation order) run up to steps[i] steps each;
+ * a serving loop gives each length a budget that takes about the same time, so blocks holding
+ * short lengths do not idle while the longest items finish. */
+int mm_b200_plan_run_each_async(mm_b200_plan *p, const size_t *steps);
+int mm_b200_plan_run_each(mm_b200_plan *p, const size_t *steps);
 void *mm_b200_plan_stream(mm_b200_plan *p);
 /* Kernel launches of the plan so far, and how many of them were graph replays. */
 uint64_t mm_b200_plan_launches(const mm_b200_plan *p);

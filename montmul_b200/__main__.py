@@ -5,7 +5,7 @@
     python -m montmul_b200 score --backend b200 [--slots S] [--label TEXT] [--csv PATH]
     python -m montmul_b200 sweep [--bits 1024 8192 ...] [--slots S] [--ebits 256]
     python -m montmul_b200 mixed [--slots 2000] [--lo 8192] [--hi 300000] [--ebits 1000]
-    python -m montmul_b200 serve [--load 0.7 0.95] [--requests 150] [--lo 10000] [--hi 200000]
+    python -m montmul_b200 serve [--load 0.7 0.95] [--duration 40] [--lo 10000] [--hi 200000]
     python -m montmul_b200 tune  [--lengths ...] [--force]
 
 bench, prp and score print `key=value` fields as the reference does (and append a CSV row with
@@ -95,7 +95,7 @@ def tribonacci(n: int) -> int:
 
 def cmd_score(a) -> int:
     """The standard score at --slots, or at the best of SMs x {1, 2, 4, 8, 16} (main.rs:192-299)."""
-    from .score import GMP_M5_SECONDS_PER_MODSQ_100K, ScoreConfig, best_slots, score
+    from .score import GMP_M5_SECONDS_PER_MODSQ_100K, ScoreConfig, best_slots, gpu_overhead, score
     dev = _backend(a.backend, a.device)
     make = lambda: dev  # noqa: E731
     if a.slots:
@@ -106,10 +106,11 @@ def cmd_score(a) -> int:
         cands = [s for s in cands if lib().mm_b200_batch_bytes(s, 8192, 63) * 1.2 < dev.free_memory()]
         slots = best_slots(make, 100_000, cands)
     s = score(make, ScoreConfig.standard(slots))
+    s.overhead = gpu_overhead(make, ScoreConfig.standard(slots))
     _emit([("timestamp", int(time.time())), ("label", '"' + a.label.replace('"', '""') + '"'),
            ("device", _device_name(dev)), ("backend", a.backend), ("slots", s.slots),
            ("modsq_per_s", f"{s.modsq_per_s:.2f}"), ("mad", f"{s.mad:.2f}"),
-           ("fermat_tests_per_hour", f"{s.fermat_tests_per_hour:.4f}"), ("overhead", ""), ("sm_pct", ""),
+           ("fermat_tests_per_hour", f"{s.fermat_tests_per_hour:.4f}"), ("overhead", f"{s.overhead:.4f}"), ("sm_pct", ""),
            ("mem_pct", ""), ("gmp_core_equiv", f"{s.modsq_per_s * GMP_M5_SECONDS_PER_MODSQ_100K:.4f}")], a.csv)
     return 0
 
@@ -146,7 +147,7 @@ def main(argv=None) -> int:
     p.add_argument("--quantum", type=int, default=1 << 16)
     p = sub.add_parser("serve", allow_abbrev=False)
     p.add_argument("--load", type=float, nargs="*", default=[0.7, 0.95])
-    p.add_argument("--requests", type=int, default=150)
+    p.add_argument("--duration", type=float, default=40.0, help="seconds of arrivals")
     p.add_argument("--lo", type=int, default=10_000)
     p.add_argument("--hi", type=int, default=200_000)
     p.add_argument("--quantum", type=int, default=128)

@@ -49,6 +49,7 @@ SIGNATURES = {
     "mm_b200_set_exponent": ([_vp, _sz, _u32p, _sz, _sz], C.c_int),
     "mm_b200_set_exponents": ([_vp, _u32p, _sz, _u32p], C.c_int),
     "mm_b200_run": ([_vp, _sz], C.c_int),
+    "mm_b200_run_bare": ([_vp, _sz], C.c_int),
     "mm_b200_mul": ([_vp, _sz, _sz, _sz], C.c_int),
     "mm_b200_read": ([_vp, _sz, _u32p], C.c_int),
     "mm_b200_read_all": ([_vp, _u32p], C.c_int),
@@ -70,12 +71,43 @@ SIGNATURES = {
     "mm_b200_plan_create": ([_vp, _sz, _sz, C.POINTER(_vp)], C.c_int),
     "mm_b200_plan_run_async": ([_vp, _sz], C.c_int),
     "mm_b200_plan_sync": ([_vp], C.c_int),
+    "mm_b200_plan_run_each_async": ([_vp, _vp], C.c_int),
+    "mm_b200_plan_run_each": ([_vp, _vp], C.c_int),
     "mm_b200_plan_run": ([_vp, _sz], C.c_int),
     "mm_b200_plan_stream": ([_vp], _vp),
     "mm_b200_plan_launches": ([_vp], C.c_uint64),
     "mm_b200_plan_graph_launches": ([_vp], C.c_uint64),
     "mm_b200_plan_destroy": ([_vp], None),
+    "mm_b200_t_upload": ([_vp, _vp, _sz, _sz, C.POINTER(_vp)], C.c_int),
+    "mm_b200_t_download_raw": ([_vp, _vp, _vp], C.c_int),
+    "mm_b200_t_forward": ([_vp, _sz, _sz], C.c_int),
+    "mm_b200_t_inverse": ([_vp, _sz, _sz], C.c_int),
+    "mm_b200_t_pointwise": ([_vp, _vp, _vp, _vp, _sz, _sz], C.c_int),
+    "mm_b200_t_load_forward": ([_vp, _vp, _sz, _sz, _sz, C.POINTER(_vp)], C.c_int),
+    "mm_b200_t_count": ([_vp], _sz),
+    "mm_b200_t_len": ([_vp], _sz),
+    "mm_b200_t_free": ([_vp], None),
 }
+
+P1, P2 = (1 << 31) - 1, (1 << 61) - 1
+_CRT_INV = pow(P2 % P1, -1, P1)
+
+
+def crt(c1: int, c2: int) -> int:
+    """The coefficient in [0, M31 M61) with residues c1 mod M31 and c2 mod M61 (field.rs:284-294)."""
+    return c2 + P2 * (((c1 - c2) * _CRT_INV) % P1)
+
+
+class TBuf:
+    """Transform-domain data of `count` vectors of one length (the Transform trait's Buf)."""
+
+    def __init__(self, ptr, length, count, owner):
+        self.ptr, self.len, self.count, self.owner = ptr, length, count, owner
+
+    def __del__(self):
+        if getattr(self, "ptr", None):
+            lib().mm_b200_t_free(self.ptr)
+            self.ptr = None
 
 
 class Schedule(C.Structure):
@@ -130,8 +162,16 @@ class _Batch:
 class B200:
     """`Gpu`-equivalent backend on one B200 (wraparound path, k = L/2)."""
 
-    def __init__(self, device: int = 0, max_launch_steps: int = 0, force_global: bool = False):
-        opts = Options(device, int(force_global), 1, max_launch_steps)
+    def __init__(self, device: int = 0, max_launch_steps: int = 0, force_global: bool = False, tuned: bool = True,
+                 wraparound: bool = True):
+        """tuned: every new batch takes its length's row of the autotuner's schedule table
+        (montmul_b200.tune), unless max_launch_steps or force_global fix the schedule.
+        wraparound: GpuOptions::wraparound (gpu/mod.rs:36-44): k = L/2 and the half-length cyclic
+        REDC (bit-identical to Cpu::with_wraparound); off, k = k0 and the plain REDC
+        (bit-identical to Cpu::default)."""
+        opts = Options(device, int(force_global), int(wraparound), max_launch_steps)
+        self._tuned = tuned and not max_launch_steps and not force_global
+        self._table = None
         ptr = _vp()
         _check(lib().mm_b200_open(C.byref(opts), C.byref(ptr)))
         self._dev = ptr
@@ -176,6 +216,13 @@ class B200:
                                     np.ascontiguousarray(two_n, np.uint32), C.byref(ptr)))
         st = _Batch(ptr, k, slots)
         st.owner = self   # keep the device open while the batch lives
+        if self._tuned:
+            from . import tune
+            if self._table is None:
+                self._table = tune.load_table()
+            sc = tune.schedule_for(self.device_name(), length, self._table)
+            if sc:
+                self.set_schedule(st, sc["global"], sc["launch_steps"], sc["step_ns"])
         return st
 
     def load(self, st, i, limbs):
@@ -196,6 +243,10 @@ class B200:
 
     def run(self, st, bits):
         _check(lib().mm_b200_run(st.ptr, bits))
+
+    def run_bare(self, st, bits):
+        """Gpu::run_bare: steps that stop after the squaring, x unchanged (gpu/mod.rs:109-111)."""
+        _check(lib().mm_b200_run_bare(st.ptr, bits))
 
     def run_async(self, st, bits):
         _check(lib().mm_b200_run_async(st.ptr, bits))
@@ -227,6 +278,55 @@ class B200:
 
     def remaining(self, st, i):
         return int(lib().mm_b200_remaining(st.ptr, i))
+
+    # The Transform trait (transform.rs:22-46; the Gpu impl, gpu/mod.rs:286-319).
+    def upload(self, coeffs, length: int, count: int) -> TBuf:
+        c = np.ascontiguousarray(coeffs, np.uint32).reshape(-1)
+        assert c.size == length * count
+        ptr = _vp()
+        _check(lib().mm_b200_t_upload(self._dev, _ptr(c), length, count, C.byref(ptr)))
+        return TBuf(ptr, length, count, self)
+
+    def download_raw(self, buf: TBuf):
+        """(f1, f2): count x L/2 x (re, im) field values in the reference's element order."""
+        n = buf.len // 2
+        f1 = np.zeros((buf.count * n, 2), np.uint32)
+        f2 = np.zeros((buf.count * n, 2), np.uint64)
+        _check(lib().mm_b200_t_download_raw(buf.ptr, _ptr(f1), _ptr(f2)))
+        return f1, f2
+
+    def download(self, buf: TBuf):
+        """Exact coefficients in [0, Q) (CRT of the two fields), count x L, row-major."""
+        f1, f2 = self.download_raw(buf)
+        n = buf.len // 2
+        out = [0] * (buf.count * buf.len)
+        for v in range(buf.count):
+            for j in range(n):
+                e = v * n + j
+                out[v * buf.len + j] = crt(int(f1[e, 0]), int(f2[e, 0]))
+                out[v * buf.len + j + n] = crt(int(f1[e, 1]), int(f2[e, 1]))
+        return out
+
+    def upload_scales(self, scales):
+        return np.ascontiguousarray(scales, np.uint32)
+
+    def forward(self, buf: TBuf, length: int, count: int) -> None:
+        _check(lib().mm_b200_t_forward(buf.ptr, length, count))
+
+    def inverse(self, buf: TBuf, length: int, count: int) -> None:
+        _check(lib().mm_b200_t_inverse(buf.ptr, length, count))
+
+    def pointwise(self, out: TBuf, a: TBuf, b: TBuf, scales, length: int, count: int) -> None:
+        sc = None if scales is None else np.ascontiguousarray(scales, np.uint32)
+        _check(lib().mm_b200_t_pointwise(out.ptr, a.ptr, b.ptr, _ptr(sc), length, count))
+
+    def load_forward(self, limbs, k: int, length: int, count: int) -> TBuf:
+        """k limbs per vector, zero-padded to the length, forward-transformed (gpu/mod.rs load_forward)."""
+        li = np.ascontiguousarray(limbs, np.uint32).reshape(-1)
+        assert li.size == k * count
+        ptr = _vp()
+        _check(lib().mm_b200_t_load_forward(self._dev, _ptr(li), k, length, count, C.byref(ptr)))
+        return TBuf(ptr, length, count, self)
 
     # Schedules and in-place refill (no counterpart in the reference's Backend trait).
     def set_schedule(self, st, global_mode: bool, launch_steps: int = 0, step_ns: float = 0.0):
@@ -280,6 +380,12 @@ class Plan:
 
     def run_async(self, bits: int) -> None:
         _check(lib().mm_b200_plan_run_async(self._p, int(bits)))
+
+    def run_each(self, steps) -> None:
+        """One launch in which the slots of batch i run up to steps[i] steps."""
+        s = np.ascontiguousarray(steps, np.uintp)
+        assert s.size == len(self._keep)
+        _check(lib().mm_b200_plan_run_each(self._p, _ptr(s)))
 
     def sync(self) -> None:
         _check(lib().mm_b200_plan_sync(self._p))

@@ -20,17 +20,22 @@ struct SlotArgs {
     const F1* tab1;
     uint32_t ew;
     uint32_t base;
+    uint32_t bare;        // 1: each step stops after T = c x^2 (x unchanged), as run_bare
+    uint32_t k;           // limbs per value (n with the wraparound path; k0 <= n without)
+    uint32_t plain;       // 1: REDC without the wraparound path (constants F(N') | F(N))
 };
 
 typedef void (*StepFn)(SlotArgs, uint32_t, uint32_t);
 typedef void (*MulFn)(SlotArgs, uint32_t, uint32_t, uint32_t, F2*, F1*);
 typedef void (*SetupFn)(const uint32_t*, const uint32_t*, F2*, F1*, const F2K*, const F1*, F2, F1, uint32_t,
-                        const uint32_t*);
+                        const uint32_t*, uint32_t, int);
+typedef void (*TransformFn)(F2*, F1*, const F2K*, const F1*, uint32_t, int);
 
 struct KernelSet {
     StepFn step;
     MulFn mul;
     SetupFn setup;
+    TransformFn transform;   // the Transform trait's forward / inverse (shared memory)
     int threads;   // block size
     int smem;      // dynamic shared memory per block
 };
@@ -45,7 +50,7 @@ struct GArgs {
 };
 typedef void (*GStepFn)(GArgs, uint32_t, uint32_t);
 typedef void (*GMulFn)(GArgs, uint32_t, uint32_t, uint32_t, F2*, F1*);
-typedef void (*GSetupFn)(GArgs, const uint32_t*, const uint32_t*, F2*, F1*, F2, F1, uint32_t, const uint32_t*);
+typedef void (*GSetupFn)(GArgs, const uint32_t*, const uint32_t*, F2*, F1*, F2, F1, uint32_t, const uint32_t*);   // k, plain in g.a
 struct GlobalKernels {
     GStepFn step;
     GMulFn mul;
@@ -59,9 +64,9 @@ GlobalKernels global_kernels();       // mm_global.cu
 // The mixed-length persistent launch (mm_mixed.cu): one descriptor per batch, one work item
 // (descriptor index, slot) per slot; blocks take items from a device counter in item order.
 struct MixedDesc {
-    GArgs g;       // the batch's slot state (w2 / w1 unused in shared mode)
-    int global;    // 1: global mode; 0: the vector in shared memory (m <= kMaxMixedSharedLogN)
-    int pad;
+    GArgs g;        // the batch's slot state (w2 / w1 unused in shared mode)
+    int global;     // 1: global mode; 0: the vector in shared memory (m <= kMaxMixedSharedLogN)
+    uint32_t bits;  // steps per item of this batch in this launch (0: the launch's `bits`)
 };
 constexpr int kMixedThreads = 256;
 constexpr int kMaxMixedSharedLogN = 12;   // 96 KiB: two blocks per SM, as global mode

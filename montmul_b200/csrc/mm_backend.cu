@@ -72,6 +72,7 @@ struct mm_b200_device {
     int max_smem = 0;
     int max_launch_steps = 512;
     bool force_global = false;
+    bool wrap = true;          // GpuOptions::wraparound (k = L/2); off: k = k0 and the plain REDC
     bool global_configured = false;
     bool mixed_configured = false;
     std::string name;
@@ -87,6 +88,7 @@ struct mm_b200_batch {
     uint32_t base = 3;
     KernelSet ks{};
     bool global = false;       // vector in HBM, tiles through shared memory (mm_global.cuh)
+    bool plain = false;        // REDC without the wraparound path (k may be below L/2)
     GlobalKernels gk{};
     F2* d_w2 = nullptr;        // global mode: slots x n work elements
     F1* d_w1 = nullptr;
@@ -155,6 +157,7 @@ int ensure_tables(mm_b200_device* dev, int m, bool global, const DevTables** out
         MM_CK(cudaFuncSetAttribute((const void*)ks.step, cudaFuncAttributeMaxDynamicSharedMemorySize, ks.smem));
         MM_CK(cudaFuncSetAttribute((const void*)ks.mul, cudaFuncAttributeMaxDynamicSharedMemorySize, ks.smem));
         MM_CK(cudaFuncSetAttribute((const void*)ks.setup, cudaFuncAttributeMaxDynamicSharedMemorySize, ks.smem));
+        MM_CK(cudaFuncSetAttribute((const void*)ks.transform, cudaFuncAttributeMaxDynamicSharedMemorySize, ks.smem));
         MM_CK(cudaFuncSetAttribute((const void*)ks.step, cudaFuncAttributePreferredSharedMemoryCarveout,
                                    cudaSharedmemCarveoutMaxShared));
         dev->configured[m] = true;
@@ -179,6 +182,9 @@ SlotArgs slot_args(const mm_b200_batch* b) {
     a.tab1 = b->tab->t1;
     a.ew = (uint32_t)b->ew;
     a.base = b->base;
+    a.bare = 0;
+    a.k = (uint32_t)b->k;
+    a.plain = b->plain ? 1 : 0;
     return a;
 }
 
@@ -258,16 +264,20 @@ int check_err(mm_b200_batch* b, const char* what) {
     return MM_OK;
 }
 
-int launch_steps(mm_b200_batch* b, size_t bits) {
+int launch_steps(mm_b200_batch* b, size_t bits, bool bare = false) {
     size_t most = 0;
     for (size_t i = 0; i < b->slots; ++i) most = std::max(most, (size_t)(b->nbits[i] - b->pos[i]));
     size_t left = std::min(bits, most);
     if (left == 0) return MM_OK;
     int rc = push(b);
     if (rc) return rc;
-    const SlotArgs a = slot_args(b);
+    SlotArgs a = slot_args(b);
+    a.bare = bare ? 1 : 0;
     GArgs g{};
-    if (b->global) g = global_args(b);
+    if (b->global) {
+        g = global_args(b);
+        g.a.bare = a.bare;
+    }
     const size_t chunk = (size_t)std::max(1, b->sched.launch_steps > 0 ? b->sched.launch_steps : b->dev->max_launch_steps);
     while (left > 0) {
         const uint32_t s = (uint32_t)std::min(left, chunk);
@@ -278,7 +288,7 @@ int launch_steps(mm_b200_batch* b, size_t bits) {
         for (size_t i = 0; i < b->slots; ++i) b->pos[i] += std::min<uint32_t>(s, b->nbits[i] - b->pos[i]);
         left -= s;
     }
-    b->host_x_valid = false;
+    if (!bare) b->host_x_valid = false;
     return MM_OK;
 }
 
@@ -372,6 +382,26 @@ int check_slot_list(const mm_b200_batch* b, size_t count, const size_t* slots, c
 // Accessors for entry points defined in other translation units.
 int mm_set_error(int code, const std::string& msg) { return fail(code, msg); }
 
+int mm_device_ordinal(const mm_b200_device* dev) { return dev ? dev->device : 0; }
+
+// The tables and kernels of length 2^(m+1) in one mode, for the Transform trait.
+int mm_device_tables(mm_b200_device* dev, int m, bool global, const F2K** t2, const F1** t1, KernelSet* ks,
+                     GlobalKernels* gk) {
+    const DevTables* t = nullptr;
+    int rc = ensure_tables(dev, m, global, &t);
+    if (rc) return rc;
+    *t2 = t->t2;
+    *t1 = t->t1;
+    if (global) {
+        *gk = global_kernels();
+    } else {
+        kernel_set(m, *ks);
+    }
+    return MM_OK;
+}
+
+int mm_batch_plain(const mm_b200_batch* b) { return b && b->plain ? 1 : 0; }
+
 int mm_batch_view(const mm_b200_batch* b, int* device, int* m, const F2** c2, const F1** c1, const F2K** tab2,
                   const F1** tab1, size_t* slots) {
     *device = b->dev->device;
@@ -392,7 +422,6 @@ int mm_b200_open(const mm_b200_options* opts, mm_b200_device** out) {
     if (!out) return fail(MM_ERR_ARG, "null output pointer");
     mm_b200_options o{0, 0, 1, 0};
     if (opts) o = *opts;
-    if (!o.wraparound) return fail(MM_ERR_UNSUPPORTED, "this backend runs the wraparound path only (k = L/2)");
     if (!host::check_fixed_roots()) return fail(MM_ERR_UNSUPPORTED, "field roots differ from the ones the kernels assume");
     int count = 0;
     MM_CK(cudaGetDeviceCount(&count));
@@ -407,6 +436,7 @@ int mm_b200_open(const mm_b200_options* opts, mm_b200_device** out) {
     d->name = prop.name;
     if (o.max_launch_steps > 0) d->max_launch_steps = o.max_launch_steps;
     d->force_global = o.force_global != 0;
+    d->wrap = o.wraparound != 0;
     *out = d;
     return MM_OK;
 }
@@ -448,7 +478,7 @@ size_t mm_b200_supported_lengths(size_t* out, size_t cap) {
     return cnt;
 }
 
-int mm_b200_full_k(const mm_b200_device*) { return 1; }
+int mm_b200_full_k(const mm_b200_device* dev) { return dev && !dev->wrap ? 0 : 1; }
 
 size_t mm_b200_batch_bytes(size_t slots, size_t len, size_t exp_words) {
     const size_t n = len / 2;
@@ -471,7 +501,8 @@ int mm_b200_create(mm_b200_device* dev, size_t k, size_t len, uint32_t base, siz
     if (len < 8 || m < kMinLogN || ((size_t)2 << m) != len) return fail(MM_ERR_ARG, "transform length must be a power of two >= 8");
     if (m > kMaxGlobalLogN) return fail(MM_ERR_UNSUPPORTED, "transform length " + std::to_string(len) + " exceeds the largest supported (2^24)");
     const bool global = m > kMaxSharedLogN || (dev->force_global && m >= kMinGlobalLogN);
-    if (k != len / 2) return fail(MM_ERR_ARG, "wraparound needs k = L/2");
+    if (dev->wrap && k != len / 2) return fail(MM_ERR_ARG, "wraparound needs k = L/2");
+    if (k == 0 || k > len / 2) return fail(MM_ERR_ARG, "k must be in 1 .. L/2");
     if (base < 1 || base > 4) return fail(MM_ERR_ARG, "base must be in 1..4 (lazy range)");
     MM_CK(cudaSetDevice(dev->device));
     // batch_bytes counts global mode's work vectors from n > 8192 on; forced global mode below
@@ -498,6 +529,7 @@ int mm_b200_create(mm_b200_device* dev, size_t k, size_t len, uint32_t base, siz
     b->base = base;
     b->tab = tab;
     b->global = global;
+    b->plain = !dev->wrap;
     b->sched.global = global ? 1 : 0;
     b->gk = global_kernels();
     b->gtab = gtab;
@@ -538,7 +570,8 @@ int mm_b200_create(mm_b200_device* dev, size_t k, size_t len, uint32_t base, siz
                                                                        gtab->inv8h2, gtab->inv8h1, (uint32_t)first, nullptr);
         else
             b->ks.setup<<<grid, b->ks.threads, b->ks.smem, b->stream>>>(d_n, d_np, b->d_c2, b->d_c1, tab->t2, tab->t1,
-                                                                       tab->inv8h2, tab->inv8h1, (uint32_t)first, nullptr);
+                                                                       tab->inv8h2, tab->inv8h1, (uint32_t)first, nullptr,
+                                                                       (uint32_t)k, b->plain ? 1 : 0);
         MM_CK(cudaGetLastError());
         ++b->launches;
     }
@@ -616,6 +649,14 @@ int mm_b200_sync(mm_b200_batch* b) {
     if (!b) return fail(MM_ERR_ARG, "sync: null batch");
     MM_CK(cudaStreamSynchronize(b->stream));
     return check_err(b, "run");
+}
+
+int mm_b200_run_bare(mm_b200_batch* b, size_t bits) {
+    if (!b) return fail(MM_ERR_ARG, "run_bare: null batch");
+    MM_CK(cudaSetDevice(b->dev->device));
+    int rc = launch_steps(b, bits, true);
+    if (rc) return rc;
+    return mm_b200_sync(b);
 }
 
 int mm_b200_run(mm_b200_batch* b, size_t bits) {
@@ -739,7 +780,8 @@ int mm_b200_set_moduli(mm_b200_batch* b, size_t count, const size_t* slots, cons
                                                                        tab->inv8h2, tab->inv8h1, 0, ids);
         else
             b->ks.setup<<<grid, b->ks.threads, b->ks.smem, b->stream>>>(nl, npl, b->d_c2, b->d_c1, tab->t2, tab->t1,
-                                                                       tab->inv8h2, tab->inv8h1, 0, ids);
+                                                                       tab->inv8h2, tab->inv8h1, 0, ids, (uint32_t)k,
+                                                                       b->plain ? 1 : 0);
         MM_CK(cudaGetLastError());
         ++b->launches;
     }
@@ -832,6 +874,8 @@ struct mm_b200_plan {
     uint32_t* d_counter = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
+    cudaGraphExec_t exec_each = nullptr;   // the launch with per-batch step budgets
+    cudaGraph_t graph_each = nullptr;
     uint64_t launches = 0, graph_launches = 0;
 };
 
@@ -845,8 +889,9 @@ double step_cost(const mm_b200_batch* b, bool global) {
     return n * (double)b->m * (global ? 1.2 : 1.0);
 }
 
-MixedDesc mixed_desc(const mm_b200_batch* b, bool global) {
+MixedDesc mixed_desc(const mm_b200_batch* b, bool global, uint32_t bits) {
     MixedDesc d{};
+    d.bits = bits;
     if (global) d.g = global_args(b);
     else {
         d.g.a = slot_args(b);
@@ -950,7 +995,7 @@ int mm_b200_plan_run_async(mm_b200_plan* p, size_t bits) {
     }
     // Descriptors follow the batches' buffers (exponent rows can be reallocated and restrided).
     std::vector<MixedDesc> d(nb);
-    for (size_t i = 0; i < nb; ++i) d[i] = mixed_desc(p->batches[i], plan_global(p->batches[i]));
+    for (size_t i = 0; i < nb; ++i) d[i] = mixed_desc(p->batches[i], plan_global(p->batches[i]), 0);
     if (std::memcmp(d.data(), p->h_descs, nb * sizeof(MixedDesc)) != 0) {
         MM_CK(cudaStreamSynchronize(p->stream));   // the pinned copy may still feed the last upload
         std::memcpy(p->h_descs, d.data(), nb * sizeof(MixedDesc));
@@ -989,6 +1034,64 @@ int mm_b200_plan_run_async(mm_b200_plan* p, size_t bits) {
     return MM_OK;
 }
 
+int mm_b200_plan_run_each_async(mm_b200_plan* p, const size_t* steps) {
+    if (!p || !steps) return fail(MM_ERR_ARG, "plan_run_each: null argument");
+    MM_CK(cudaSetDevice(p->dev->device));
+    const size_t nb = p->batches.size();
+    bool any = false;
+    for (size_t i = 0; i < nb; ++i) {
+        if (steps[i] > 0xffffffffu) return fail(MM_ERR_ARG, "plan_run_each: steps must be below 2^32");
+        const mm_b200_batch* b = p->batches[i];
+        for (size_t s = 0; steps[i] && s < b->slots && !any; ++s) any = b->pos[s] < b->nbits[s];
+    }
+    if (!any) return MM_OK;
+    for (size_t i = 0; i < nb; ++i) {
+        mm_b200_batch* b = p->batches[i];
+        int rc = push(b);
+        if (rc) return rc;
+        MM_CK(cudaEventRecord(p->ready[i], b->stream));
+        MM_CK(cudaStreamWaitEvent(p->stream, p->ready[i], 0));
+    }
+    // The launch's own `bits` is 0, so a batch whose budget is 0 runs no step.
+    std::vector<MixedDesc> d(nb);
+    for (size_t i = 0; i < nb; ++i) d[i] = mixed_desc(p->batches[i], plan_global(p->batches[i]), (uint32_t)steps[i]);
+    if (std::memcmp(d.data(), p->h_descs, nb * sizeof(MixedDesc)) != 0) {
+        MM_CK(cudaStreamSynchronize(p->stream));
+        std::memcpy(p->h_descs, d.data(), nb * sizeof(MixedDesc));
+        MM_CK(cudaMemcpyAsync(p->d_descs, p->h_descs, nb * sizeof(MixedDesc), cudaMemcpyHostToDevice, p->stream));
+    }
+    if (!p->exec_each) {
+        MM_CK(cudaStreamBeginCapture(p->stream, cudaStreamCaptureModeThreadLocal));
+        int rc = plan_enqueue(p, 0);
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamEndCapture(p->stream, &g);
+        if (rc) return rc;
+        if (e != cudaSuccess) return fail(MM_ERR_CUDA, std::string("plan capture: ") + cudaGetErrorString(e));
+        p->graph_each = g;
+        MM_CK(cudaGraphInstantiate(&p->exec_each, p->graph_each, 0));
+    }
+    MM_CK(cudaGraphLaunch(p->exec_each, p->stream));
+    ++p->graph_launches;
+    ++p->launches;
+    for (size_t i = 0; i < nb; ++i) {
+        mm_b200_batch* b = p->batches[i];
+        for (size_t s = 0; s < b->slots; ++s)
+            b->pos[s] += (uint32_t)std::min<size_t>(steps[i], (size_t)(b->nbits[s] - b->pos[s]));
+    }
+    MM_CK(cudaEventRecord(p->done, p->stream));
+    for (auto* b : p->batches) {
+        MM_CK(cudaStreamWaitEvent(b->stream, p->done, 0));
+        b->host_x_valid = false;
+    }
+    return MM_OK;
+}
+
+int mm_b200_plan_run_each(mm_b200_plan* p, const size_t* steps) {
+    int rc = mm_b200_plan_run_each_async(p, steps);
+    if (rc) return rc;
+    return mm_b200_plan_sync(p);
+}
+
 int mm_b200_plan_sync(mm_b200_plan* p) {
     if (!p) return fail(MM_ERR_ARG, "plan_sync: null plan");
     MM_CK(cudaSetDevice(p->dev->device));
@@ -1016,6 +1119,8 @@ void mm_b200_plan_destroy(mm_b200_plan* p) {
     if (p->stream) cudaStreamSynchronize(p->stream);
     if (p->exec) cudaGraphExecDestroy(p->exec);
     if (p->graph) cudaGraphDestroy(p->graph);
+    if (p->exec_each) cudaGraphExecDestroy(p->exec_each);
+    if (p->graph_each) cudaGraphDestroy(p->graph_each);
     cudaFree(p->d_items);
     cudaFree(p->d_descs);
     cudaFree(p->d_counter);

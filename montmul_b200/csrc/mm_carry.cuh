@@ -162,6 +162,86 @@ __device__ __noinline__ void carry_low_and_pack(F2* s2, F1* s1, uint64_t* sc) {
     __syncthreads();
 }
 
+// m = the low k limbs of a product whose low n coefficients are the real parts of the first n
+// elements (k <= n), written to `out` (global); the REDC without the wraparound path
+// (cpu.rs:459-462).
+template <int M, int NT>
+__device__ __noinline__ void carry_low_to(const F2* s2, const F1* s1, uint32_t* __restrict__ out, int k, uint64_t* sc) {
+    constexpr int N = 1 << M, COUNT = N;
+    constexpr int E = cmax(2, COUNT / NT), TA = COUNT / E;
+    const int t = threadIdx.x;
+    uint32_t L[E];
+    uint64_t c = 0;
+    const int q0 = t * E;
+    if (t < TA) {
+        Acc96 acc;
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            uint32_t w0, w1, w2;
+            crt3(s1[swz(q0 + e)].re, s2[swz(q0 + e)].re, w0, w1, w2);
+            L[e] = acc.add_shift(w0, w1, w2);
+        }
+        c = acc.rest();
+    } else {
+#pragma unroll
+        for (int e = 0; e < E; ++e) L[e] = 0;
+    }
+    block_resolve<E, TA, NT>(L, c, 0, sc);   // limbs from k on are dropped (mod R)
+    if (t < TA) {
+#pragma unroll
+        for (int e = 0; e < E; ++e)
+            if (q0 + e < k) out[q0 + e] = L[e];
+    }
+    __syncthreads();
+}
+
+// x = (T + m N) / R without the wraparound path (cpu.rs:470-481): the product m N in natural
+// order (coefficient q < n in the real part of element q, q >= n in the imaginary part of element
+// q - n) plus T's high half from limb k, plus `flag` (T mod R != 0: the low halves sum to R
+// then) at limb k; limbs k .. 2k - 1 into x. Returns false when anything remains above them.
+template <int M, int NT>
+__device__ __noinline__ bool carry_shift_add(const F2* s2, const F1* s1, const uint32_t* __restrict__ tl,
+                                             uint32_t* __restrict__ x, int k, uint32_t flag, uint64_t* sc) {
+    constexpr int N = 1 << M, COUNT = 2 * N;
+    constexpr int E = cmax(2, COUNT / NT), TA = COUNT / E;
+    const int t = threadIdx.x;
+    uint32_t L[E];
+    uint64_t c = 0;
+    const int q0 = t * E;
+    if (t < TA) {
+        const bool hi = q0 >= N;
+        const int j0 = hi ? q0 - N : q0;
+        Acc96 acc;
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            const int q = q0 + e;
+            const F2 a2 = s2[swz(j0 + e)];
+            const F1 a1 = s1[swz(j0 + e)];
+            uint32_t w0, w1, w2;
+            crt3(hi ? a1.im : a1.re, hi ? a2.im : a2.re, w0, w1, w2);
+            const uint64_t add = (q >= k && q < 2 * k ? (uint64_t)tl[q] : 0u) + (q == k ? flag : 0u);
+            const uint64_t lo = (((uint64_t)w1 << 32) | w0) + add;
+            w2 += lo < add;
+            L[e] = acc.add_shift((uint32_t)lo, (uint32_t)(lo >> 32), w2);
+        }
+        c = acc.rest();
+    } else {
+#pragma unroll
+        for (int e = 0; e < E; ++e) L[e] = 0;
+    }
+    const uint64_t top = block_resolve<E, TA, NT>(L, c, 0, sc);
+    int stray = 0;
+    if (t < TA) {
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            const int q = q0 + e;
+            if (q >= k && q < 2 * k) x[q - k] = L[e];
+            else if (q >= 2 * k) stray |= L[e] != 0;
+        }
+    }
+    return !__syncthreads_or(stray) && top == 0;
+}
+
 // x = floor(T / R) + ((cyclic + T mod R) mod (R - 1)) with the cyclic product m N mod (R - 1)
 // packed in the first n/2 elements (coefficient q: element q/2, re for even q, im for odd q),
 // T (2n limbs) in global memory; writes x (n limbs). cpu.rs:297-328. Returns false when the

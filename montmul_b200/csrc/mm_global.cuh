@@ -183,6 +183,34 @@ __device__ __noinline__ void g_dit_last(F2* v2, F1* v1, const F2K* t2, const F1*
     __syncthreads();
 }
 
+// Weighted first global pass of complex elements in place (the Transform trait's forward, as
+// dif_first_complex).
+template <int R, int NT>
+__device__ __noinline__ void g_dif_first_complex(F2* v2, F1* v1, const F2K* t2, const F1* t1, const F2K* cin2,
+                                                 const F1* cin1, int lq) {
+    const int q = 1 << lq;
+#pragma unroll 1
+    for (int j = threadIdx.x; j < q; j += NT) {
+        {
+            F2 x[R];
+#pragma unroll
+            for (int k = 0; k < R; ++k) x[k] = lkmul(v2[swz(j + k * q)], cin2[k]);
+            ldif<R>(x);
+#pragma unroll
+            for (int k = 0; k < R; ++k) v2[swz(j + k * q)] = lkmul(lcfold(x[k]), t2[k * q + j]);
+        }
+        {
+            F1 x[R];
+#pragma unroll
+            for (int k = 0; k < R; ++k) x[k] = cmul(v1[swz(j + k * q)], cin1[k]);
+            bf_dif<R, F1>(x);
+#pragma unroll
+            for (int k = 0; k < R; ++k) v1[swz(j + k * q)] = cmul(x[k], t1[k * q + j]);
+        }
+    }
+    __syncthreads();
+}
+
 template <int NT>
 __device__ __forceinline__ void g_dif_first_rt(int R, const uint32_t* lim, int cnt, F2* v2, F1* v1, const F2K* t2,
                                                const F1* t1, const F2K* c2, const F1* c1, int lq) {
@@ -202,11 +230,11 @@ __device__ __forceinline__ void g_dit_last_rt(int R, F2* v2, F1* v1, const F2K* 
 // already in place (unweighted), and DIT down to natural order.
 template <int NT>
 __device__ __forceinline__ void g_fwd(int m, bool weighted, const uint32_t* lim, F2* v2, F1* v1, const F2K* tab2,
-                                      const F1* tab1) {
+                                      const F1* tab1, int cnt = 0) {
     const int P = gl_passes(m), n = 1 << m;
     int i = 0;
     if (weighted) {
-        g_dif_first_rt<NT>(gl_radix(m, 0), lim, n, v2, v1, tab2 + gl_fwd_off(m, 0, true), tab1 + gl_fwd_off(m, 0, true),
+        g_dif_first_rt<NT>(gl_radix(m, 0), lim, cnt ? cnt : n, v2, v1, tab2 + gl_fwd_off(m, 0, true), tab1 + gl_fwd_off(m, 0, true),
                            tab2 + gl_in_const_off(m, true), tab1 + gl_in_const_off(m, true), gl_lq(m, 0));
         i = 1;
     }
@@ -423,6 +451,67 @@ __device__ __noinline__ void half_pointwise_rt(F2* v2, F1* v1, int H, const F2* 
     __syncthreads();
 }
 
+// ---- the REDC without the wraparound path on global vectors ----
+// m = the low k limbs of the product's real parts (k <= n) into out, as carry_low_to.
+template <int NT>
+__device__ __noinline__ void g_carry_low_to(const F2* v2, const F1* v1, int n, uint32_t* out, int k, uint64_t* sc) {
+    uint64_t cin = 0;
+#pragma unroll 1
+    for (int base = 0; base < k; base += kChunkE * NT) {
+        const int q0 = base + threadIdx.x * kChunkE;
+        uint32_t L[kChunkE];
+        Acc96 acc;
+#pragma unroll
+        for (int e = 0; e < kChunkE; ++e) {
+            uint32_t w0 = 0, w1 = 0, w2 = 0;
+            if (q0 + e < n) {
+                const int el = swz(q0 + e);
+                crt3(v1[el].re, v2[el].re, w0, w1, w2);
+            }
+            L[e] = acc.add_shift(w0, w1, w2);
+        }
+        cin = block_resolve<kChunkE, NT, NT>(L, acc.rest(), cin, sc);
+#pragma unroll
+        for (int e = 0; e < kChunkE; ++e)
+            if (q0 + e < k) out[q0 + e] = L[e];
+    }
+    __syncthreads();
+}
+
+// x = (T + m N) / R, as carry_shift_add, in chunks over the 2n coefficients of m N.
+template <int NT>
+__device__ __noinline__ bool g_carry_shift_add(const F2* v2, const F1* v1, int n, const uint32_t* tl, uint32_t* x, int k,
+                                               uint32_t flag, uint64_t* sc) {
+    int stray = 0;
+    uint64_t cin = 0;
+#pragma unroll 1
+    for (int base = 0; base < 2 * n; base += kChunkE * NT) {
+        const int q0 = base + threadIdx.x * kChunkE;
+        uint32_t L[kChunkE];
+        Acc96 acc;
+#pragma unroll
+        for (int e = 0; e < kChunkE; ++e) {
+            const int q = q0 + e;
+            const bool hi = q >= n;
+            const int el = swz(hi ? q - n : q);
+            uint32_t w0, w1, w2;
+            crt3(hi ? v1[el].im : v1[el].re, hi ? v2[el].im : v2[el].re, w0, w1, w2);
+            const uint64_t add = (q >= k && q < 2 * k ? (uint64_t)tl[q] : 0u) + (q == k ? flag : 0u);
+            const uint64_t lo = (((uint64_t)w1 << 32) | w0) + add;
+            w2 += lo < add;
+            L[e] = acc.add_shift((uint32_t)lo, (uint32_t)(lo >> 32), w2);
+        }
+        cin = block_resolve<kChunkE, NT, NT>(L, acc.rest(), cin, sc);
+#pragma unroll
+        for (int e = 0; e < kChunkE; ++e) {
+            const int q = q0 + e;
+            if (q >= k && q < 2 * k) x[q - k] = L[e];
+            else if (q >= 2 * k) stray |= L[e] != 0;
+        }
+    }
+    return !__syncthreads_or(stray) && cin == 0;
+}
+
 // ---- the wraparound steps on global vectors ----
 enum { kStepOk = 0, kStepCarry = 1, kStepTimeout = 2 };
 
@@ -454,6 +543,29 @@ __device__ __forceinline__ int g_redc_wrap(F2* w2, F1* w1, int m, const uint32_t
     return g_wrap_combine<NT>(w2, w1, n, tl, x, sc) ? kStepOk : kStepCarry;
 }
 
+// REDC without the wraparound path in global mode (as redc_plain). Returns a kStep* status.
+template <int NT>
+__device__ __forceinline__ int g_redc_plain(F2* w2, F1* w1, int m, const uint32_t* tl, uint32_t* x, const F2* cc2,
+                                            const F1* cc1, const F2K* tab2, const F1* tab1, uint64_t* sc,
+                                            const TileSmem& sm, uint32_t& par, int k) {
+    const int n = 1 << m;
+    const F2K* tt2 = tab2 + glt_tile_off(m);
+    const F1* tt1 = tab1 + glt_tile_off(m);
+    int nz = 0;
+    for (int q = threadIdx.x; q < k; q += NT) nz |= tl[q] != 0;
+    const uint32_t flag = __syncthreads_or(nz) ? 1u : 0u;
+    g_fwd<NT>(m, true, tl, w2, w1, tab2, tab1, k);
+    if (!tile_phase<NT>(w2, w1, n, tt2, tt1, SpecMulRT{cc2, cc1, n / 8}, kTileFull, sm, par)) return kStepTimeout;
+    par = tile_par_next(par, n);
+    g_inv<NT, true>(m, true, w2, w1, tab2, tab1);
+    g_carry_low_to<NT>(w2, w1, n, x, k, sc);
+    g_fwd<NT>(m, true, x, w2, w1, tab2, tab1, k);
+    if (!tile_phase<NT>(w2, w1, n, tt2, tt1, SpecMulRT{cc2 + n, cc1 + n, n / 8}, kTileFull, sm, par)) return kStepTimeout;
+    par = tile_par_next(par, n);
+    g_inv<NT, false>(m, true, w2, w1, tab2, tab1);
+    return g_carry_shift_add<NT>(w2, w1, n, tl, x, k, flag, sc) ? kStepOk : kStepCarry;
+}
+
 // Up to `bits` steps on one slot, global mode (as step_slot). `par` carries the mbarrier
 // parities from one call to the next. Returns false (on every thread) after a bulk copy that did
 // not complete in time; the parities are then no longer usable.
@@ -461,8 +573,8 @@ template <int NT>
 __device__ __forceinline__ bool gstep_slot(const GArgs& g, uint32_t slot, uint32_t bits, const TileSmem& sm, uint64_t* sc,
                                            uint32_t& par) {
     const SlotArgs& a = g.a;
-    const int m = g.m, n = 1 << m;
-    uint32_t* x = a.x + (size_t)slot * n;
+    const int m = g.m, n = 1 << m, k = (int)a.k;
+    uint32_t* x = a.x + (size_t)slot * k;
     uint32_t* tl = a.tbuf + (size_t)slot * 2 * n;
     const F2* cc2 = a.c2 + (size_t)slot * 2 * n;
     const F1* cc1 = a.c1 + (size_t)slot * 2 * n;
@@ -478,12 +590,14 @@ __device__ __forceinline__ bool gstep_slot(const GArgs& g, uint32_t slot, uint32
     for (uint32_t it = 0; it < bits && pos < nb; ++it, ++pos) {
         const uint32_t bit = (ex[pos >> 5] >> (31 - (pos & 31))) & 1;
         const uint32_t c = bit ? a.base : 1;
-        g_fwd<NT>(m, true, x, w2, w1, a.tab2, a.tab1);
+        g_fwd<NT>(m, true, x, w2, w1, a.tab2, a.tab1, k);
         if (!tile_phase<NT>(w2, w1, n, tt2, tt1, SquareOp{c}, kTileFull, sm, par)) { st = kStepTimeout; break; }
         par = tile_par_next(par, n);
         g_inv<NT, false>(m, true, w2, w1, a.tab2, a.tab1);
         carry_ok &= g_carry_product<NT>(w2, w1, n, tl, sc) == 0;
-        st = g_redc_wrap<NT>(w2, w1, m, tl, x, cc2, cc1, a.tab2, a.tab1, sc, sm, par);
+        if (a.bare) continue;
+        st = a.plain ? g_redc_plain<NT>(w2, w1, m, tl, x, cc2, cc1, a.tab2, a.tab1, sc, sm, par, k)
+                     : g_redc_wrap<NT>(w2, w1, m, tl, x, cc2, cc1, a.tab2, a.tab1, sc, sm, par);
         if (st == kStepTimeout) break;
         carry_ok &= st == kStepOk;
     }
@@ -524,17 +638,21 @@ __global__ void __launch_bounds__(NT, 2) gmul_kernel(GArgs g, uint32_t out, uint
     const F1* tt1 = a.tab1 + glt_tile_off(m);
     uint32_t par = 0;
     int st = kStepTimeout;
-    g_fwd<NT>(m, true, a.x + (size_t)ib * n, w2, w1, a.tab2, a.tab1);
+    const int k = (int)a.k;
+    g_fwd<NT>(m, true, a.x + (size_t)ib * k, w2, w1, a.tab2, a.tab1, k);
     if (tile_phase<NT>(w2, w1, n, tt2, tt1, SpecStoreRT{spec2, spec1, n / 8}, kTileDifOp, sm, par)) {
         par = tile_par_next(par, n);
-        g_fwd<NT>(m, true, a.x + (size_t)ia * n, w2, w1, a.tab2, a.tab1);
+        g_fwd<NT>(m, true, a.x + (size_t)ia * k, w2, w1, a.tab2, a.tab1, k);
         if (tile_phase<NT>(w2, w1, n, tt2, tt1, SpecMulRT{spec2, spec1, n / 8}, kTileFull, sm, par)) {
             par = tile_par_next(par, n);
             g_inv<NT, false>(m, true, w2, w1, a.tab2, a.tab1);
             uint32_t* tl = a.tbuf + (size_t)out * 2 * n;
             const bool fits = g_carry_product<NT>(w2, w1, n, tl, sc) == 0;
-            st = g_redc_wrap<NT>(w2, w1, m, tl, a.x + (size_t)out * n, a.c2 + (size_t)out * 2 * n,
-                                 a.c1 + (size_t)out * 2 * n, a.tab2, a.tab1, sc, sm, par);
+            uint32_t* xo = a.x + (size_t)out * k;
+            const F2* oc2 = a.c2 + (size_t)out * 2 * n;
+            const F1* oc1 = a.c1 + (size_t)out * 2 * n;
+            st = a.plain ? g_redc_plain<NT>(w2, w1, m, tl, xo, oc2, oc1, a.tab2, a.tab1, sc, sm, par, k)
+                         : g_redc_wrap<NT>(w2, w1, m, tl, xo, oc2, oc1, a.tab2, a.tab1, sc, sm, par);
             if (st == kStepOk && !fits) st = kStepCarry;
         }
     }
@@ -562,10 +680,21 @@ __global__ void __launch_bounds__(NT, 2) gsetup_kernel(GArgs g, const uint32_t* 
     const F1* tt1 = a.tab1 + glt_tile_off(m);
     uint32_t par = 0;
     bool ok = false;
-    g_fwd<NT>(m, true, npl + row * n, w2, w1, a.tab2, a.tab1);
+    const int k = (int)a.k;
+    g_fwd<NT>(m, true, npl + row * k, w2, w1, a.tab2, a.tab1, k);
+    if (a.plain) {
+        // F(N) in the second half (cpu.rs:518-521).
+        if (tile_phase<NT>(w2, w1, n, tt2, tt1, SpecStoreRT{o2, o1, n / 8}, kTileDifOp, sm, par)) {
+            par = tile_par_next(par, n);
+            g_fwd<NT>(m, true, nl + row * k, w2, w1, a.tab2, a.tab1, k);
+            ok = tile_phase<NT>(w2, w1, n, tt2, tt1, SpecStoreRT{o2 + n, o1 + n, n / 8}, kTileDifOp, sm, par);
+        }
+        if (threadIdx.x == 0 && !ok) a.err[slot] = kErrTimeout;
+        return;
+    }
     if (tile_phase<NT>(w2, w1, n, tt2, tt1, SpecStoreRT{o2, o1, n / 8}, kTileDifOp, sm, par)) {
         par = tile_par_next(par, n);
-        pack_pairs(nl + row * n, w2, w1, h, NT);
+        pack_pairs(nl + row * k, w2, w1, h, NT);
         const F2K* ht2 = a.tab2 + glt_half_off(m);
         const F1* ht1 = a.tab1 + glt_half_off(m);
         if (m - 1 > kTileLog) g_fwd<NT>(m - 1, false, nullptr, w2, w1, ht2, ht1);
@@ -576,6 +705,44 @@ __global__ void __launch_bounds__(NT, 2) gsetup_kernel(GArgs g, const uint32_t* 
         }
     }
     if (threadIdx.x == 0 && !ok) a.err[slot] = kErrTimeout;
+}
+
+// The Transform trait's forward or inverse of vector first + blockIdx.x in global mode, in place
+// in a device buffer in the kernels' element order; the result is canonical. A bulk copy that
+// does not complete in time sets err[0] to 2.
+template <int NT>
+__global__ void __launch_bounds__(NT, 2) gtransform_kernel(F2* v2, F1* v1, const F2K* tab2, const F1* tab1, int m,
+                                                           uint32_t first, int inverse, uint32_t* err) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ uint64_t bars[2];
+    const TileSmem sm{smem_raw, bars};
+    tile_init(sm);
+    const int n = 1 << m, P = gl_passes(m);
+    F2* w2 = v2 + (size_t)(first + blockIdx.x) * n;
+    F1* w1 = v1 + (size_t)(first + blockIdx.x) * n;
+    const F2K* tt2 = tab2 + glt_tile_off(m);
+    const F1* tt1 = tab1 + glt_tile_off(m);
+    bool ok;
+    if (!inverse) {
+        const int R0 = gl_radix(m, 0), lq0 = gl_lq(m, 0);
+        const F2K* t2 = tab2 + gl_fwd_off(m, 0, true);
+        const F1* t1 = tab1 + gl_fwd_off(m, 0, true);
+        const F2K* c2 = tab2 + gl_in_const_off(m, true);
+        const F1* c1 = tab1 + gl_in_const_off(m, true);
+        if (R0 == 8) g_dif_first_complex<8, NT>(w2, w1, t2, t1, c2, c1, lq0);
+        else if (R0 == 4) g_dif_first_complex<4, NT>(w2, w1, t2, t1, c2, c1, lq0);
+        else g_dif_first_complex<2, NT>(w2, w1, t2, t1, c2, c1, lq0);
+        for (int i = 1; i < P; ++i)
+            g_pass<NT>(gl_radix(m, i), true, w2, w1, tab2 + gl_fwd_off(m, i, true), tab1 + gl_fwd_off(m, i, true),
+                       gl_lq(m, i), n);
+        ok = tile_phase<NT>(w2, w1, n, tt2, tt1, SquareOp{1}, kTileDif, sm, 0);
+    } else {
+        ok = tile_phase<NT>(w2, w1, n, tt2, tt1, SquareOp{1}, kTileDit, sm, 0);
+        if (ok) g_inv<NT, false>(m, true, w2, w1, tab2, tab1);
+    }
+    if (ok)
+        for (int e = threadIdx.x; e < n; e += NT) w2[e] = lccanon(w2[e]);
+    if (threadIdx.x == 0 && !ok) *err = kErrTimeout;
 }
 
 }  // namespace mm

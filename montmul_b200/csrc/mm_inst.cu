@@ -13,7 +13,8 @@ namespace mm {
 
 KernelSet MM_CAT(kernels_m, MM_M)() {
     constexpr int NT = threads_for(MM_M);
-    return KernelSet{step_kernel<MM_M, NT>, mul_kernel<MM_M, NT>, setup_kernel<MM_M, NT>, NT, smem_bytes<MM_M>()};
+    return KernelSet{step_kernel<MM_M, NT>, mul_kernel<MM_M, NT>, setup_kernel<MM_M, NT>, transform_kernel<MM_M, NT>, NT,
+                     smem_bytes<MM_M>()};
 }
 
 }  // namespace mm

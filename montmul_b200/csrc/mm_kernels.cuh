@@ -163,6 +163,42 @@ __device__ __forceinline__ void half_factors_block(F2* s2, F1* s1, int H, const 
     __syncthreads();
 }
 
+// The Transform trait's forward (weight by zeta^j, DIF) or inverse (DIT, unweight by
+// zeta^-j / n) of vector first + blockIdx.x, in place in a device buffer whose element order is
+// the kernels' (element j at swz(j)); the result is canonical (cpu.rs:86-103, 349-407).
+template <int M, int NT>
+__global__ void __launch_bounds__(NT) transform_kernel(F2* v2, F1* v1, const F2K* tab2, const F1* tab1, uint32_t first,
+                                                       int inverse) {
+    constexpr int N = 1 << M, P = sched_passes(M);
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    F2* s2 = reinterpret_cast<F2*>(smem_raw);
+    F1* s1 = reinterpret_cast<F1*>(smem_raw + 16 * N);
+    F2* g2 = v2 + (size_t)(first + blockIdx.x) * N;
+    F1* g1 = v1 + (size_t)(first + blockIdx.x) * N;
+    for (int e = threadIdx.x; e < N; e += NT) {
+        s2[e] = g2[e];
+        s1[e] = g1[e];
+    }
+    __syncthreads();
+    if (!inverse) {
+        dif_first_complex<M, NT>(s2, s1, tab2, tab1);
+        if constexpr (P >= 2) smem_pass<M, (P >= 2 ? 1 : 0), true, NT, true>(s2, s1, tab2, tab1);
+        if constexpr (P >= 3) smem_pass<M, (P >= 3 ? 2 : 0), true, NT, true>(s2, s1, tab2, tab1);
+        if constexpr (P >= 4) smem_pass<M, (P >= 4 ? 3 : 0), true, NT, true>(s2, s1, tab2, tab1);
+        if constexpr (P >= 5) smem_pass<M, (P >= 5 ? 4 : 0), true, NT, true>(s2, s1, tab2, tab1);
+    } else {
+        if constexpr (P >= 5) smem_pass<M, (P >= 5 ? 4 : 0), false, NT, true>(s2, s1, tab2, tab1);
+        if constexpr (P >= 4) smem_pass<M, (P >= 4 ? 3 : 0), false, NT, true>(s2, s1, tab2, tab1);
+        if constexpr (P >= 3) smem_pass<M, (P >= 3 ? 2 : 0), false, NT, true>(s2, s1, tab2, tab1);
+        if constexpr (P >= 2) smem_pass<M, (P >= 2 ? 1 : 0), false, NT, true>(s2, s1, tab2, tab1);
+        dit_last_complex<M, NT>(s2, s1, tab2, tab1);
+    }
+    for (int e = threadIdx.x; e < N; e += NT) {
+        g2[e] = lccanon(s2[e]);
+        g1[e] = s1[e];
+    }
+}
+
 // Shared memory of one block: F2 vector (16 n B), F1 vector (8 n B).
 template <int M> constexpr int smem_bytes() { return 24 << M; }
 
@@ -184,15 +220,38 @@ __device__ __noinline__ bool redc_wrap(F2* s2, F1* s1, const uint32_t* tl, uint3
     return wrap_combine<M, NT>(s2, s1, tl, x, sc);
 }
 
+// REDC without the wraparound path (cpu.rs:453-484 with half = None), k <= n limbs: m = (T mod R)
+// N' mod R through F(N'), then m N through F(N) (both in cc, fused-pass order), and
+// x = T_high + (m N)_high + [T mod R != 0]. m overwrites x, which the step no longer needs.
+template <int M, int NT>
+__device__ __noinline__ bool redc_plain(F2* s2, F1* s1, const uint32_t* tl, uint32_t* x, const F2* cc2, const F1* cc1,
+                                        const F2K* tab2, const F1* tab1, uint64_t* sc, int k) {
+    constexpr int N = 1 << M;
+    int nz = 0;
+    for (int q = threadIdx.x; q < k; q += NT) nz |= tl[q] != 0;
+    const uint32_t flag = __syncthreads_or(nz) ? 1u : 0u;
+    fwd_limbs<M, NT>(tl, k, s2, s1, tab2, tab1);
+    fused_mid<M, NT, true>(tl, k, s2, s1, tab2, tab1, SpecMulOp<M>{cc2, cc1});
+    inv_to_natural<M, NT, true>(s2, s1, tab2, tab1);
+    carry_low_to<M, NT>(s2, s1, x, k, sc);
+    fwd_limbs<M, NT>(x, k, s2, s1, tab2, tab1);
+    fused_mid<M, NT, false>(x, k, s2, s1, tab2, tab1, SpecMulOp<M>{cc2 + N, cc1 + N});
+    inv_to_natural<M, NT, false>(s2, s1, tab2, tab1);
+    return carry_shift_add<M, NT>(s2, s1, tl, x, k, flag, sc);
+}
+
 // Up to `bits` steps x <- x^2 c^bit R^-1 on one slot (cpu.rs:543-556), the whole block, the
 // vector in `smem_raw` (24 n bytes). Used by the uniform launch and the mixed-length launch.
+// With a.bare each step ends after T = c x^2 and x stays as it was (the reference's run_bare,
+// lib.rs:883-927, which times the squaring alone).
 template <int M, int NT>
 __device__ __forceinline__ void step_slot(const SlotArgs& a, uint32_t slot, uint32_t bits, unsigned char* smem_raw,
                                           uint64_t* sc) {
     constexpr int N = 1 << M;
     F2* s2 = reinterpret_cast<F2*>(smem_raw);
     F1* s1 = reinterpret_cast<F1*>(smem_raw + 16 * N);
-    uint32_t* x = a.x + (size_t)slot * N;
+    const int k = (int)a.k;
+    uint32_t* x = a.x + (size_t)slot * k;
     uint32_t* tl = a.tbuf + (size_t)slot * 2 * N;
     const F2* cc2 = a.c2 + (size_t)slot * 2 * N;
     const F1* cc1 = a.c1 + (size_t)slot * 2 * N;
@@ -203,11 +262,13 @@ __device__ __forceinline__ void step_slot(const SlotArgs& a, uint32_t slot, uint
     for (uint32_t it = 0; it < bits && pos < nb; ++it, ++pos) {
         const uint32_t bit = (ex[pos >> 5] >> (31 - (pos & 31))) & 1;
         const uint32_t c = bit ? a.base : 1;
-        fwd_limbs<M, NT>(x, N, s2, s1, a.tab2, a.tab1);
-        fused_mid<M, NT, false>(x, N, s2, s1, a.tab2, a.tab1, SquareOp{c});
+        fwd_limbs<M, NT>(x, k, s2, s1, a.tab2, a.tab1);
+        fused_mid<M, NT, false>(x, k, s2, s1, a.tab2, a.tab1, SquareOp{c});
         inv_to_natural<M, NT, false>(s2, s1, a.tab2, a.tab1);
         ok &= carry_product<M, NT>(s2, s1, tl, sc) == 0;
-        ok &= redc_wrap<M, NT>(s2, s1, tl, x, cc2, cc1, a.tab2, a.tab1, sc);
+        if (a.bare) continue;
+        if (a.plain) ok &= redc_plain<M, NT>(s2, s1, tl, x, cc2, cc1, a.tab2, a.tab1, sc, k);
+        else ok &= redc_wrap<M, NT>(s2, s1, tl, x, cc2, cc1, a.tab2, a.tab1, sc);
     }
     __syncthreads();   // every thread has read pos before it is written
     if (threadIdx.x == 0) {
@@ -233,18 +294,23 @@ __global__ void __launch_bounds__(NT) mul_kernel(SlotArgs a, uint32_t out, uint3
     F2* s2 = reinterpret_cast<F2*>(smem_raw);
     F1* s1 = reinterpret_cast<F1*>(smem_raw + 16 * N);
     __shared__ uint64_t sc[CarryScratch<NT>::words];
-    const uint32_t* xb = a.x + (size_t)ib * N;
-    const uint32_t* xa = a.x + (size_t)ia * N;
-    fwd_limbs<M, NT>(xb, N, s2, s1, a.tab2, a.tab1);
-    fused_mid<M, NT, false>(xb, N, s2, s1, a.tab2, a.tab1, SpecStoreOp<M>{spec2, spec1});
+    const int k = (int)a.k;
+    const uint32_t* xb = a.x + (size_t)ib * k;
+    const uint32_t* xa = a.x + (size_t)ia * k;
+    fwd_limbs<M, NT>(xb, k, s2, s1, a.tab2, a.tab1);
+    fused_mid<M, NT, false>(xb, k, s2, s1, a.tab2, a.tab1, SpecStoreOp<M>{spec2, spec1});
     __syncthreads();
-    fwd_limbs<M, NT>(xa, N, s2, s1, a.tab2, a.tab1);
-    fused_mid<M, NT, false>(xa, N, s2, s1, a.tab2, a.tab1, SpecMulOp<M>{spec2, spec1});
+    fwd_limbs<M, NT>(xa, k, s2, s1, a.tab2, a.tab1);
+    fused_mid<M, NT, false>(xa, k, s2, s1, a.tab2, a.tab1, SpecMulOp<M>{spec2, spec1});
     inv_to_natural<M, NT, false>(s2, s1, a.tab2, a.tab1);
     uint32_t* tl = a.tbuf + (size_t)out * 2 * N;
     bool ok = carry_product<M, NT>(s2, s1, tl, sc) == 0;
-    ok &= redc_wrap<M, NT>(s2, s1, tl, a.x + (size_t)out * N, a.c2 + (size_t)out * 2 * N, a.c1 + (size_t)out * 2 * N,
-                           a.tab2, a.tab1, sc);
+    uint32_t* xo = a.x + (size_t)out * k;
+    if (a.plain)
+        ok &= redc_plain<M, NT>(s2, s1, tl, xo, a.c2 + (size_t)out * 2 * N, a.c1 + (size_t)out * 2 * N, a.tab2, a.tab1,
+                                sc, k);
+    else
+        ok &= redc_wrap<M, NT>(s2, s1, tl, xo, a.c2 + (size_t)out * 2 * N, a.c1 + (size_t)out * 2 * N, a.tab2, a.tab1, sc);
     if (threadIdx.x == 0 && !ok) a.err[out] = 1;
 }
 
@@ -256,21 +322,28 @@ __global__ void __launch_bounds__(NT) mul_kernel(SlotArgs a, uint32_t out, uint3
 template <int M, int NT>
 __global__ void __launch_bounds__(NT) setup_kernel(const uint32_t* nl, const uint32_t* npl, F2* c2, F1* c1, const F2K* tab2,
                                                    const F1* tab1, F2 inv8h2, F1 inv8h1, uint32_t first,
-                                                   const uint32_t* slots) {
+                                                   const uint32_t* slots, uint32_t k, int plain) {
     constexpr int N = 1 << M, H = N / 2;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     F2* s2 = reinterpret_cast<F2*>(smem_raw);
     F1* s1 = reinterpret_cast<F1*>(smem_raw + 16 * N);
-    // Rows of nl / npl: all slots from `first` on, or (with a slot list) one row per listed slot.
+    // Rows of nl / npl (k limbs each): all slots from `first` on, or (with a slot list) one row
+    // per listed slot.
     const uint32_t slot = slots ? slots[blockIdx.x] : first + blockIdx.x;
     const size_t row = slots ? blockIdx.x : slot;
-    const uint32_t* np = npl + row * N;
-    const uint32_t* nn = nl + row * N;
+    const uint32_t* np = npl + row * k;
+    const uint32_t* nn = nl + row * k;
     F2* o2 = c2 + (size_t)slot * 2 * N;
     F1* o1 = c1 + (size_t)slot * 2 * N;
-    fwd_limbs<M, NT>(np, N, s2, s1, tab2, tab1);
-    fused_mid<M, NT, false>(np, N, s2, s1, tab2, tab1, SpecStoreOp<M>{o2, o1});
+    fwd_limbs<M, NT>(np, (int)k, s2, s1, tab2, tab1);
+    fused_mid<M, NT, false>(np, (int)k, s2, s1, tab2, tab1, SpecStoreOp<M>{o2, o1});
     __syncthreads();
+    if (plain) {
+        // F(N) in the second half (cpu.rs:518-521), in fused-pass order.
+        fwd_limbs<M, NT>(nn, (int)k, s2, s1, tab2, tab1);
+        fused_mid<M, NT, false>(nn, (int)k, s2, s1, tab2, tab1, SpecStoreOp<M>{o2 + N, o1 + N});
+        return;
+    }
     pack_pairs(nn, s2, s1, H, NT);
     const F2K* ht2 = tab2 + lt_half_off(M);
     const F1* ht1 = tab1 + lt_half_off(M);

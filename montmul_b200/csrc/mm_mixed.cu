@@ -38,22 +38,23 @@ __global__ void __launch_bounds__(kMixedThreads, 2)
         if (i >= count) break;
         const uint2 it = items[i];
         const MixedDesc& d = descs[it.x];
+        const uint32_t steps = d.bits ? d.bits : bits;
         if (d.global) {
-            if (!gstep_slot<kMixedThreads>(d.g, it.y, bits, sm, sc, par)) break;
+            if (!gstep_slot<kMixedThreads>(d.g, it.y, steps, sm, sc, par)) break;
             continue;
         }
         switch (d.g.m) {
-            case 2: mixed_shared<2>(d.g.a, it.y, bits, smem_raw, sc); break;
-            case 3: mixed_shared<3>(d.g.a, it.y, bits, smem_raw, sc); break;
-            case 4: mixed_shared<4>(d.g.a, it.y, bits, smem_raw, sc); break;
-            case 5: mixed_shared<5>(d.g.a, it.y, bits, smem_raw, sc); break;
-            case 6: mixed_shared<6>(d.g.a, it.y, bits, smem_raw, sc); break;
-            case 7: mixed_shared<7>(d.g.a, it.y, bits, smem_raw, sc); break;
-            case 8: mixed_shared<8>(d.g.a, it.y, bits, smem_raw, sc); break;
-            case 9: mixed_shared<9>(d.g.a, it.y, bits, smem_raw, sc); break;
-            case 10: mixed_shared<10>(d.g.a, it.y, bits, smem_raw, sc); break;
-            case 11: mixed_shared<11>(d.g.a, it.y, bits, smem_raw, sc); break;
-            case 12: mixed_shared<12>(d.g.a, it.y, bits, smem_raw, sc); break;
+            case 2: mixed_shared<2>(d.g.a, it.y, steps, smem_raw, sc); break;
+            case 3: mixed_shared<3>(d.g.a, it.y, steps, smem_raw, sc); break;
+            case 4: mixed_shared<4>(d.g.a, it.y, steps, smem_raw, sc); break;
+            case 5: mixed_shared<5>(d.g.a, it.y, steps, smem_raw, sc); break;
+            case 6: mixed_shared<6>(d.g.a, it.y, steps, smem_raw, sc); break;
+            case 7: mixed_shared<7>(d.g.a, it.y, steps, smem_raw, sc); break;
+            case 8: mixed_shared<8>(d.g.a, it.y, steps, smem_raw, sc); break;
+            case 9: mixed_shared<9>(d.g.a, it.y, steps, smem_raw, sc); break;
+            case 10: mixed_shared<10>(d.g.a, it.y, steps, smem_raw, sc); break;
+            case 11: mixed_shared<11>(d.g.a, it.y, steps, smem_raw, sc); break;
+            case 12: mixed_shared<12>(d.g.a, it.y, steps, smem_raw, sc); break;
             default: break;   // the host never builds such a descriptor
         }
     }

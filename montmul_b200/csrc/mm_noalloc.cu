@@ -117,6 +117,7 @@ static int noalloc_setup(int device, unsigned char** scratch, std::string& msg) 
 extern "C++" int mm_batch_view(const mm_b200_batch* b, int* device, int* m, const mm::F2** c2, const mm::F1** c1,
                                const mm::F2K** tab2, const mm::F1** tab1, size_t* slots);
 extern "C++" int mm_set_error(int code, const std::string& msg);
+extern "C++" int mm_batch_plain(const mm_b200_batch* b);
 
 extern "C" int mm_b200_mul_noalloc(const mm_b200_batch* b, size_t slot, const uint32_t* d_a, const uint32_t* d_b,
                                    uint32_t* d_out, uint32_t* d_err, void* stream) {
@@ -127,6 +128,7 @@ extern "C" int mm_b200_mul_noalloc(const mm_b200_batch* b, size_t slot, const ui
     const F1 *c1 = nullptr, *tab1 = nullptr;
     size_t slots = 0;
     if (!b || !d_a || !d_b || !d_out) return mm_set_error(MM_ERR_ARG, "mul_noalloc: null argument");
+    if (mm_batch_plain(b)) return mm_set_error(MM_ERR_UNSUPPORTED, "mul_noalloc: needs the wraparound path (k = L/2)");
     mm_batch_view(b, &device, &m, &c2, &c1, &tab2, &tab1, &slots);
     if (slot >= slots) return mm_set_error(MM_ERR_ARG, "mul_noalloc: bad slot");
     if (device < 0 || device >= kNoAllocMaxDevices) return mm_set_error(MM_ERR_ARG, "mul_noalloc: device ordinal too large");

@@ -285,6 +285,65 @@ __device__ __noinline__ void dit_last_weighted(F2* s2, F1* s1, const F2K* tab2, 
     __syncthreads();
 }
 
+// ---- the Transform trait's weighted passes on complex elements (cpu.rs:86-103) ----
+// Forward: element j + k q times zeta^(q k) before the butterfly; zeta^j and the pass twiddles
+// after it, from the table (none when the transform is this single pass, q = 1). The vector is
+// in shared memory at swz positions, canonical or reduced.
+template <int M, int NT>
+__device__ __noinline__ void dif_first_complex(F2* s2, F1* s1, const F2K* tab2, const F1* tab1) {
+    constexpr int R = sched_radix(M, 0), Q = sched_q(M, 0);
+    constexpr int toff = tab_fwd_off(M, 0, true), coff = tab_in_const_off(M, true);
+#pragma unroll 1
+    for (int j = threadIdx.x; j < Q; j += NT) {
+        {
+            F2 x[R];
+#pragma unroll
+            for (int k = 0; k < R; ++k) x[k] = lkmul(s2[swz(j + k * Q)], tab2[coff + k]);
+            ldif<R>(x);
+#pragma unroll
+            for (int k = 0; k < R; ++k)
+                s2[swz(j + k * Q)] = Q > 1 ? lkmul(lcfold(x[k]), tab2[toff + k * Q + j]) : lcfold(x[k]);
+        }
+        {
+            F1 x[R];
+#pragma unroll
+            for (int k = 0; k < R; ++k) x[k] = cmul(s1[swz(j + k * Q)], tab1[coff + k]);
+            bf_dif<R, F1>(x);
+#pragma unroll
+            for (int k = 0; k < R; ++k) s1[swz(j + k * Q)] = Q > 1 ? cmul(x[k], tab1[toff + k * Q + j]) : x[k];
+        }
+    }
+    __syncthreads();
+}
+
+// Inverse: the pass twiddles (with zeta^-j) before the butterfly, zeta^-(q k) / n after it.
+template <int M, int NT>
+__device__ __noinline__ void dit_last_complex(F2* s2, F1* s1, const F2K* tab2, const F1* tab1) {
+    constexpr int R = sched_radix(M, 0), Q = sched_q(M, 0);
+    constexpr int toff = tab_inv_off(M, 0, true), coff = tab_out_const_off(M, true);
+#pragma unroll 1
+    for (int j = threadIdx.x; j < Q; j += NT) {
+        {
+            F2 x[R];
+#pragma unroll
+            for (int k = 0; k < R; ++k)
+                x[k] = Q > 1 ? lkmul(s2[swz(j + k * Q)], tab2[toff + k * Q + j]) : s2[swz(j + k * Q)];
+            ldit<R>(x);
+#pragma unroll
+            for (int k = 0; k < R; ++k) s2[swz(j + k * Q)] = lkmul(x[k], tab2[coff + k]);
+        }
+        {
+            F1 x[R];
+#pragma unroll
+            for (int k = 0; k < R; ++k) x[k] = Q > 1 ? cmul(s1[swz(j + k * Q)], tab1[toff + k * Q + j]) : s1[swz(j + k * Q)];
+            bf_dit<R, F1>(x);
+#pragma unroll
+            for (int k = 0; k < R; ++k) s1[swz(j + k * Q)] = cmul(x[k], tab1[coff + k]);
+        }
+    }
+    __syncthreads();
+}
+
 // ---- the fused middle: last DIF pass (span 1), a pointwise operation, first DIT pass ----
 // OP::apply2/apply1(x, g) transforms the R spectrum values of group g (positions R g + k).
 // With a single pass (M <= 3) the same pass is also the weighted first/last pass.

@@ -117,6 +117,29 @@ def score(make: Callable, cfg: ScoreConfig, timer: Optional[Callable] = None) ->
     return Score(cfg.slots, m, mad(rates), m * 3600.0 / cfg.bits)
 
 
+def gpu_overhead(make: Callable, cfg: ScoreConfig) -> float:
+    """Median time of run over that of run_bare on the score workload (score.rs:140-159): the cost
+    of a whole step relative to its squaring."""
+    moduli, exps = workload(cfg)
+    batch = ModBatch(make(), moduli, 3)
+    be, st = batch.backend_and_state()
+
+    def timed(bare: bool) -> float:
+        arm(batch, exps)
+        t = time.perf_counter()
+        if bare:
+            be.run_bare(st, cfg.ebits)
+        else:
+            batch.run(cfg.ebits)
+        return time.perf_counter() - t
+
+    timed(False)
+    timed(True)
+    full = [timed(False) for _ in range(cfg.repeats)]
+    bare = [timed(True) for _ in range(cfg.repeats)]
+    return median(full) / median(bare)
+
+
 def best_slots(make: Callable, bits: int, candidates) -> int:
     """The candidate slot count with the highest score at ebits = 200, one repeat (score.rs:125-136)."""
     if not candidates:

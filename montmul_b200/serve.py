@@ -5,15 +5,17 @@ Requests arrive as a Poisson process. Each transform length has a lane: uniform 
 ("segments") whose slots keep their Montgomery state and exponent on the device. A request is
 admitted as soon as a slot of its length is free; a lane grows by one segment while the device
 memory budget allows (admission by the per-slot bytes of its length), else the request waits.
-Every tick runs `quantum` steps on every busy slot of every lane in one mixed-length plan launch
-(persistent blocks over a device work queue, replayed from a CUDA graph), then reads back the
-slots that finished and refills them in place with waiting requests: the batch is never drained.
+Every tick is one mixed-length plan launch over every busy slot of every lane (persistent blocks
+over a device work queue, replayed from a CUDA graph): the costliest length runs `quantum` steps
+and every other length the steps that take as long (from the tuned cost per step), so no block
+idles while the longest items finish. Then the slots that finished are read back and refilled in
+place with waiting requests: the batch is never drained.
 
 A Fermat request loads 1, sets the exponent N - 1 and reports the verdict x == 1; a mul request
 (a b mod N) takes two slots of the same modulus and one mul launch. Each request's time to
 verdict runs from its arrival to the tick that read its result.
 
-    python -m montmul_b200 serve [--load 0.7 0.95] [--requests 150] [--lo 10000] [--hi 200000]
+    python -m montmul_b200 serve [--load 0.7 0.95] [--duration 40] [--lo 10000] [--hi 200000]
 """
 from __future__ import annotations
 
@@ -108,6 +110,9 @@ class Server:
         self.tuned = tuned
         self.steps_done = 0
         self.ticks = []           # (t, busy slots, slot-steps run)
+        from . import tune
+        self.table = tune.load_table().get(dev.device_name(), {})
+        self.seg_steps = []       # per plan batch: steps of one tick
 
     # ---- admission ----
     def _grow(self, length: int) -> Optional[Segment]:
@@ -176,16 +181,36 @@ class Server:
         m = b.moduli[slots[0]]
         r.value = gmp.mulmod(b.read_raw_slots(slots[:1])[0], m.rinv, m.n)
         r.done = time.perf_counter() - self.t0
+        self.completed += 1
         seg.free.extend(slots)
 
     # ---- ticks ----
+    def mixed_step_ns(self, length: int) -> float:
+        """Cost of one slot-step of a length in the mixed launch, from the tuned table: shared
+        mode up to L = 8192, global mode above (the mixed launch's blocks hold 96 KiB)."""
+        row = self.table.get(str(length))
+        if not row:
+            n = length // 2
+            return float(n * max(1, n.bit_length() - 1))
+        if length > 8192:
+            g = [c["step_ns"] for c in row.get("candidates", []) if c["global"]]
+            if g:
+                return min(g)
+        return row["step_ns"]
+
     def _plan(self):
         from .backend import Plan
         if self.plan is None or self.plan_dirty:
             if self.plan is not None:
                 self.plan.close()
-            segs = [s.batch for segs in self.lanes.values() for s in segs]
-            self.plan = Plan(segs, self.quantum)
+            segs = [s for L in sorted(self.lanes) for s in self.lanes[L]]
+            self.plan = Plan([s.batch for s in segs], self.quantum)
+            self.plan_segs = segs
+            # Every length gets the steps that take as long as `quantum` steps of the costliest
+            # one, so no block idles while the longest items of a tick finish.
+            costs = [self.mixed_step_ns(s.batch.params.len) for s in segs]
+            top = max(costs)
+            self.seg_steps = [max(1, int(round(self.quantum * top / c))) for c in costs]
             self.plan_dirty = False
         return self.plan
 
@@ -196,11 +221,10 @@ class Server:
         """One quantum on every busy slot, then the finished slots are read and freed."""
         plan = self._plan()
         run = 0
-        for segs in self.lanes.values():
-            for seg in segs:
-                for s in seg.active:
-                    run += min(self.quantum, seg.batch.remaining(s))
-        plan.run(self.quantum)
+        for seg, steps in zip(self.plan_segs, self.seg_steps):
+            for s in seg.active:
+                run += min(steps, seg.batch.remaining(s))
+        plan.run_each(self.seg_steps)
         now = time.perf_counter() - self.t0
         self.steps_done += run
         self.ticks.append((now, self.busy(), run))
@@ -226,21 +250,19 @@ class Server:
         pending = deque(sorted(reqs, key=lambda r: r.arrival))
         waiting = deque()
         self.t0 = time.perf_counter()
-        left = len(reqs)
-        while left:
+        self.completed = 0
+        while self.completed < len(reqs):
             now = time.perf_counter() - self.t0
             while pending and pending[0].arrival <= now:
                 waiting.append(pending.popleft())
-            before = sum(1 for r in reqs if r.done is not None)
             if waiting:
                 self.admit(waiting, now)
             if self.busy():
-                self.tick()
+                self.completed += self.tick()
             elif pending and not waiting:
                 time.sleep(max(0.0, min(0.05, pending[0].arrival - (time.perf_counter() - self.t0))))
             elif waiting and not self.busy():
                 raise MontMulError("a request fits no lane within the memory budget")
-            left -= sum(1 for r in reqs if r.done is not None) - before
         return reqs
 
     def close(self):
@@ -260,19 +282,50 @@ def capacity(reqs, step_s) -> float:
 _LENGTHS = [1 << e for e in range(3, 25)]
 
 
-def check(reqs, threads: int = 32) -> int:
-    """Every verdict against GMP's pow_mod(3, N - 1, N) == 1, every mul against a b mod N."""
-    def one(r):
+def check(dev, reqs, gmp_bits: int = 20_000, sample: int = 24, seed: int = 2027, threads: int = 32) -> dict:
+    """Checks the served results: every mul against a b mod N; every Fermat verdict of at most
+    `gmp_bits` bits against GMP's pow_mod(3, N - 1, N) == 1 (GMP takes minutes per test at 200,000
+    bits); every known prime must be a PRP; and `sample` seeded larger requests are run again
+    alone, one uniform batch per length, and must end with the same raw Montgomery limbs (the
+    uniform batches are the path the test suite pins to the reference Cpu backend)."""
+    out = {"mul": 0, "gmp": 0, "primes": 0, "alone": 0}
+    for r in reqs:
         if r.kind == "mul":
             if r.value != r.a * r.b % r.n:
                 raise MontMulError(f"request {r.rid}: mul disagrees")
-        else:
-            want = gmp.powm(3, r.n - 1, r.n) == 1
-            if r.verdict != want or (r.prime and not r.verdict):
-                raise MontMulError(f"request {r.rid} ({r.n.bit_length()} bits): verdict {r.verdict}, pow_mod {want}")
+            out["mul"] += 1
+        elif r.prime:
+            if not r.verdict:
+                raise MontMulError(f"request {r.rid}: the prime 2^{r.n.bit_length()} - 1 was not a PRP")
+            out["primes"] += 1
+    small = [r for r in reqs if r.kind == "fermat" and r.n.bit_length() <= gmp_bits]
+
+    def one(r):
+        if r.verdict != (gmp.powm(3, r.n - 1, r.n) == 1):
+            raise MontMulError(f"request {r.rid} ({r.n.bit_length()} bits): verdict disagrees with pow_mod")
         return 1
+
     with ThreadPoolExecutor(threads) as ex:
-        return sum(ex.map(one, reqs))
+        out["gmp"] = sum(ex.map(one, small))
+    big = [r for r in reqs if r.kind == "fermat" and r.n.bit_length() > gmp_bits]
+    rng = gmp.RandState(seed)
+    picked = []
+    while big and len(picked) < sample:
+        picked.append(big.pop(rng.random_below(len(big))))
+    by_len = {}
+    for r in picked:
+        by_len.setdefault(r.length, []).append(r)
+    for group in by_len.values():
+        b = ModBatch(dev, [r.n for r in group], 3)
+        b.load_all([1] * len(group))
+        b.set_exponents([r.n - 1 for r in group])
+        while any(b.remaining(i) for i in range(len(group))):
+            b.run(1 << 20)
+        for i, r in enumerate(group):
+            if b.read_raw(i) != r.raw:
+                raise MontMulError(f"request {r.rid}: served result differs from the same test run alone")
+            out["alone"] += 1
+    return out
 
 
 def percentile(v, q: float) -> float:
@@ -315,30 +368,32 @@ def main(args) -> dict:
     from .backend import B200
     from . import tune
     dev = B200(device=args.device)
+    lengths = dev.supported_lengths()
     # Seconds per slot-step at full occupancy per length (the tuned table, measured if absent).
-    per = tune.tune(dev, sorted({Params.for_bits(b, dev.supported_lengths()).len
-                                 for b in (args.lo, args.hi)} | {1 << e for e in range(10, 15)}), log=lambda *_: None)
+    need = sorted({Params.for_bits(b, lengths).len for b in (args.lo, args.hi)} | {1 << e for e in range(10, 15)})
+    per = tune.tune(dev, [L for L in need if args.lo <= 16 * L and L <= 2 * Params.for_bits(args.hi, lengths).len],
+                    log=lambda *_: None)
 
     def step_s(length):
         return per[str(length)]["step_ns"] * 1e-9
 
-    probe = stream(args.requests, 1.0, args.lo, args.hi, seed=args.seed)
+    probe = stream(2000, 1.0, args.lo, args.hi, seed=args.seed)
     cap = capacity(probe, step_s)
-    # The plain uniform-batch rate of the same mix: total steps over their uniform-batch time.
+    # The plain uniform-batch rate of the same mix: its steps over their uniform-batch time.
     ferm = [r for r in probe if r.kind == "fermat"]
     uniform = sum(r.n.bit_length() for r in ferm) / sum(
-        r.n.bit_length() * step_s(Params.for_bits(r.n.bit_length(), dev.supported_lengths()).len) for r in ferm)
+        r.n.bit_length() * step_s(Params.for_bits(r.n.bit_length(), lengths).len) for r in ferm)
     results = []
     for load in args.load:
         rate = load * cap
-        reqs = stream(args.requests, rate, args.lo, args.hi, seed=args.seed)
+        count = max(8, int(round(rate * args.duration)))
+        reqs = stream(count, rate, args.lo, args.hi, seed=args.seed)
         srv = Server(dev, quantum=args.quantum)
         srv.serve(reqs)
         srv.close()
-        checked = check(reqs) if not args.no_check else 0
         s = summarize(srv, reqs, uniform, rate, cap)
-        s["checked"] = checked
+        s["checked"] = check(dev, reqs) if not args.no_check else None
         results.append(s)
-    return {"workload": f"{args.requests} requests, bits log-uniform in [{args.lo}, {args.hi}], "
-                        f"10% Mersenne primes, 5% mul, Poisson arrivals (seed {args.seed})",
+    return {"workload": f"Poisson arrivals for {args.duration} s, bits log-uniform in [{args.lo}, {args.hi}], "
+                        f"10% Mersenne primes, 5% mul, full base-3 Fermat tests (seed {args.seed})",
             "loads": results}

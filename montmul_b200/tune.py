@@ -13,7 +13,9 @@ It records the winner's time per slot-step (step_ns), which also orders the work
 mixed-length launch. The fixed parts of a schedule are reported beside it: threads per block,
 the radix schedule of the length-n transform, the tile length of global mode and the blocks per
 SM. The table is JSON keyed by device name, cached at $MONTMUL_B200_SCHEDULES or
-~/.cache/montmul_b200/schedules.json:
+~/.cache/montmul_b200/schedules.json; without a cache the table shipped in the package
+(montmul_b200/schedules.json, measured on a B200 with this command) applies. B200 batches take
+their length's row at creation.
 
     python -m montmul_b200.tune [--lengths 8192 16384 ...] [--force]
 """
@@ -29,6 +31,10 @@ TILE = 2048           # global mode's tile length (elements of n)
 MAX_SHARED_N = 8192   # n <= 8192 fits the shared-memory kernels
 MIN_GLOBAL_N = 4096   # global mode from n = 4096 (L = 8192)
 LAUNCH_STEPS = (64, 512)
+
+
+# The table measured on a B200 and shipped with the package; used when no cache exists.
+PACKAGED = os.path.join(os.path.dirname(os.path.abspath(__file__)), "schedules.json")
 
 
 def cache_path() -> str:
@@ -124,11 +130,14 @@ def tune_length(dev, length: int, budget_s: float = 4.0):
 
 
 def load_table():
-    try:
-        with open(cache_path()) as f:
-            return json.load(f)
-    except (OSError, ValueError):
-        return {}
+    """The cached table, or the packaged one when there is no cache."""
+    for p in (cache_path(), PACKAGED):
+        try:
+            with open(p) as f:
+                return json.load(f)
+        except (OSError, ValueError):
+            continue
+    return {}
 
 
 def save_table(table) -> None:

@@ -91,3 +91,35 @@ def test_cli_score_appends_to_csv(tmp_path):
     lines = path.read_text().splitlines()
     assert len(lines) == 3
     assert lines[0].startswith("timestamp,label,device") and ",b200,1," in lines[1]
+
+
+@pytest.mark.parametrize("bits", [5000, 100_000, 400_000])
+def test_run_bare_leaves_x_and_advances(dev, bits):
+    """Gpu::run_bare (gpu/mod.rs:109-111; lib.rs:883-927): the squaring alone, x unchanged, the
+    position advanced; run then continues from the later exponent bits."""
+    rng = RandState(31)
+    moduli = [common.rand_odd(rng, bits) for _ in range(3)]
+    exps = [common.rand_exponent(rng, 20) for _ in range(3)]
+    b = ModBatch(dev, moduli, 3)
+    b.load_all([7, 8, 9])
+    b.set_exponents(exps)
+    before = [b.read_raw(i) for i in range(3)]
+    be, st = b.backend_and_state()
+    be.run_bare(st, 10)
+    assert [b.remaining(i) for i in range(3)] == [10, 10, 10]
+    assert [b.read_raw(i) for i in range(3)] == before
+    b.run(10)
+    for i, (n, e) in enumerate(zip(moduli, exps)):
+        x = 7 + i
+        for bit in bin(e)[2:][10:]:
+            x = x * x % n
+            if bit == "1":
+                x = x * 3 % n
+        assert b.read(i) == x
+
+
+def test_overhead_ratio(dev):
+    """score.rs:140-159 on a small score workload: a whole step costs more than its squaring."""
+    from montmul_b200.score import ScoreConfig, gpu_overhead
+    r = gpu_overhead(lambda: dev, ScoreConfig(bits=100_000, slots=296, ebits=200, repeats=3, seed=2026))
+    assert 1.5 < r < 6.0

@@ -170,3 +170,21 @@ def test_refill_between_plan_runs(dev):
             if j == 0 and i == 2:
                 continue
             assert bs[j].read(i) == powm(base, exps[i], moduli[i])
+
+
+def test_plan_run_each_budgets(dev):
+    """plan.run_each: per-batch step budgets in one launch, 0 leaving a batch untouched."""
+    from montmul_b200.backend import Plan
+    spec = _batches(dev, [5000, 60_000, 250_000], 3, 50, 23)
+    bs = _arm(dev, spec)
+    plan = Plan(bs, 16)
+    plan.run_each([40, 0, 7])
+    assert [bs[0].remaining(i) for i in range(3)] == [10] * 3
+    assert [bs[1].remaining(i) for i in range(3)] == [50] * 3
+    assert [bs[2].remaining(i) for i in range(3)] == [43] * 3
+    plan.run_each([40, 50, 43])
+    plan.run(1)   # nothing left: no launch
+    for (moduli, exps, base), b in zip(spec, bs):
+        for i in range(3):
+            assert b.remaining(i) == 0 and b.read(i) == powm(base, exps[i], moduli[i])
+    assert plan.graph_launches() == 2

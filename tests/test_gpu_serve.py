@@ -42,7 +42,12 @@ def test_served_stream_same_as_alone(dev):
         if r.prime:
             assert r.verdict
         assert r.raw == _alone_raw(dev, r.n), f"request {r.rid} ({r.n.bit_length()} bits)"
-    assert serve.check(reqs) == len(reqs)
+    c = serve.check(dev, reqs, gmp_bits=20_000, sample=5)
+    ferm = [r for r in reqs if r.kind == "fermat"]
+    assert c["mul"] == len(reqs) - len(ferm)
+    assert c["primes"] == sum(1 for r in ferm if r.prime)
+    assert c["gmp"] == sum(1 for r in ferm if r.n.bit_length() <= 20_000)
+    assert c["alone"] == min(5, sum(1 for r in ferm if r.n.bit_length() > 20_000))
 
 
 def test_fermat_driver_on_mersenne_primes(dev):
