@@ -120,7 +120,18 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(rows)}
 
 
-def dist_init():
+def dist_backend() -> str:
+    """NCCL between GPUs; gloo where there is no GPU (the multi-rank path's CPU tests);
+    $MONTMUL_DIST_BACKEND overrides."""
+    b = os.environ.get("MONTMUL_DIST_BACKEND")
+    if b:
+        return b
+    import torch
+    return "nccl" if torch.cuda.is_available() else "gloo"
+
+
+def dist_init(timeout_s: float = 600.0):
+    """One process per GPU (torchrun): world size, rank and local rank from the environment."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -128,19 +139,29 @@ def dist_init():
         import datetime
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        backend = dist_backend()
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=timeout_s))
     return world, rank, local
 
 
 def allmax(v: float, world: int) -> float:
+    """The maximum of v over the ranks (every rank calls it at the same point)."""
     if world == 1:
         return v
     import torch
     import torch.distributed as dist
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    device = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([v], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def shard(slots: int, world: int, rank: int):
+    """Rank r runs slots [r * slots, (r + 1) * slots) of one seeded stream: independent moduli per
+    rank, no data exchanged (weak scaling)."""
+    return rank * slots, (rank + 1) * slots
 
 
 def barrier(world: int):
@@ -212,9 +233,10 @@ def main(argv=None):
     args = ap.parse_args(argv)
     if args.warmup < 3:
         ap.error("at least 3 warm-up steps")
-    world, rank, local = dist_init()
     if args.impl == "reference":
-        return run_reference(args, world, rank)
+        # The CPU reference arm needs no process group: rank 0 alone runs it.
+        return run_reference(args, int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")))
+    world, rank, local = dist_init()
 
     import ctypes as C
 
@@ -229,10 +251,13 @@ def main(argv=None):
     lib = bk.lib()
 
     # Workload of the largest candidate; smaller batches use its first slots (same GMP stream).
+    # With several ranks each takes its own slice of the stream.
     cands = [sms * f for f in (1, 2, 4, 8, 16)]
     cands = [s for s in cands if lib.mm_b200_batch_bytes(s, 8192, 63) * 1.2 < dev.free_memory()]
-    moduli_all, exps_all = workload(ScoreConfig(bits=BITS, slots=max(cands + [args.slots]), ebits=EBITS,
-                                                repeats=1, seed=SEED))
+    per_rank = max(cands + [args.slots])
+    moduli_w, exps_w = workload(ScoreConfig(bits=BITS, slots=per_rank * world, ebits=EBITS, repeats=1, seed=SEED))
+    lo, hi = shard(per_rank, world, rank)
+    moduli_all, exps_all = moduli_w[lo:hi], exps_w[lo:hi]
 
     def make_batch(slots):
         return ModBatch(dev, moduli_all[:slots], 3)
@@ -269,6 +294,7 @@ def main(argv=None):
                 best = (s, rate)
             del b
         slots = best[0]
+    slots = int(allmax(float(slots), world))   # every rank runs the same slot count
 
     batch = make_batch(slots)
     exps = exps_all[:slots]
