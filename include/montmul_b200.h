@@ -196,6 +196,13 @@ int mm_b200_plan_run(mm_b200_plan *p, size_t bits);
  * short lengths do not idle while the longest items finish. */
 int mm_b200_plan_run_each_async(mm_b200_plan *p, const size_t *steps);
 int mm_b200_plan_run_each(mm_b200_plan *p, const size_t *steps);
+/* One launch over an explicit work list, taken in list order: item i runs up to steps[i]
+ * (>= 1) steps of slot slot[i] of batch batch[i]; each slot at most once. A scheduler orders the
+ * list longest first and sizes the budgets so the plan's resident blocks (plan_blocks) finish
+ * together. Waits for the launch and checks errors, as plan_run. */
+int mm_b200_plan_run_items(mm_b200_plan *p, size_t count, const uint32_t *batch, const uint32_t *slot,
+                           const uint32_t *steps);
+int mm_b200_plan_blocks(const mm_b200_plan *p);
 void *mm_b200_plan_stream(mm_b200_plan *p);
 /* Kernel launches of the plan so far, and how many of them were graph replays. */
 uint64_t mm_b200_plan_launches(const mm_b200_plan *p);

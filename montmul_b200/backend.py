@@ -73,6 +73,8 @@ SIGNATURES = {
     "mm_b200_plan_sync": ([_vp], C.c_int),
     "mm_b200_plan_run_each_async": ([_vp, _vp], C.c_int),
     "mm_b200_plan_run_each": ([_vp, _vp], C.c_int),
+    "mm_b200_plan_run_items": ([_vp, _sz, _vp, _vp, _vp], C.c_int),
+    "mm_b200_plan_blocks": ([_vp], C.c_int),
     "mm_b200_plan_run": ([_vp, _sz], C.c_int),
     "mm_b200_plan_stream": ([_vp], _vp),
     "mm_b200_plan_launches": ([_vp], C.c_uint64),
@@ -380,6 +382,19 @@ class Plan:
 
     def run_async(self, bits: int) -> None:
         _check(lib().mm_b200_plan_run_async(self._p, int(bits)))
+
+    def run_items(self, batch, slot, steps) -> None:
+        """One launch over an explicit list: item i runs up to steps[i] steps of slot slot[i]
+        of batch batch[i] (each slot at most once), taken in list order."""
+        b = np.ascontiguousarray(batch, np.uint32)
+        s = np.ascontiguousarray(slot, np.uint32)
+        t = np.ascontiguousarray(steps, np.uint32)
+        assert b.size == s.size == t.size and (t.size == 0 or t.min() >= 1)
+        _check(lib().mm_b200_plan_run_items(self._p, b.size, _ptr(b), _ptr(s), _ptr(t)))
+
+    def blocks(self) -> int:
+        """Resident blocks of the plan's launch (items that run at once)."""
+        return int(lib().mm_b200_plan_blocks(self._p))
 
     def run_each(self, steps) -> None:
         """One launch in which the slots of batch i run up to steps[i] steps."""

@@ -71,7 +71,9 @@ struct MixedDesc {
 constexpr int kMixedThreads = 256;
 constexpr int kMaxMixedSharedLogN = 12;   // 96 KiB: two blocks per SM, as global mode
 constexpr int kMixedSmem = 24 << kMaxMixedSharedLogN;
-typedef void (*MixedFn)(const MixedDesc*, const uint2*, uint32_t, uint32_t*, uint32_t);
+// Items: (descriptor, slot, steps, unused); steps 0 takes the descriptor's, then the launch's.
+// The item count is read from device memory, so one captured launch serves any list.
+typedef void (*MixedFn)(const MixedDesc*, const uint4*, const uint32_t*, uint32_t*, uint32_t);
 MixedFn mixed_kernel();               // mm_mixed.cu
 
 // Threads per block for transform length 2^m: one radix-8 group per thread up to 256 threads.

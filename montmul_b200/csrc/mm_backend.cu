@@ -869,8 +869,14 @@ struct mm_b200_plan {
     int grid = 0;
     MixedDesc* d_descs = nullptr;
     MixedDesc* h_descs = nullptr;     // pinned copy of what the device holds
-    uint2* d_items = nullptr;
+    uint4* d_items = nullptr;          // every slot, longest first (plan_run, plan_run_each)
     uint32_t count = 0;
+    uint32_t* d_count = nullptr;       // [0]: count of d_items; [1]: count of the tick list
+    uint4* d_tick = nullptr;           // plan_run_items' list
+    uint4* h_tick = nullptr;           // pinned staging of that list (+ its count)
+    size_t tick_cap = 0;
+    cudaGraph_t graph_items = nullptr;
+    cudaGraphExec_t exec_items = nullptr;
     uint32_t* d_counter = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -908,7 +914,8 @@ bool plan_global(const mm_b200_batch* b) { return b->global || b->m > kMaxMixedS
 // One launch of `bits` steps: the counter reset and the persistent kernel.
 int plan_enqueue(mm_b200_plan* p, uint32_t bits) {
     MM_CK(cudaMemsetAsync(p->d_counter, 0, 4, p->stream));
-    mixed_kernel()<<<p->grid, kMixedThreads, kMixedSmem, p->stream>>>(p->d_descs, p->d_items, p->count, p->d_counter, bits);
+    mixed_kernel()<<<p->grid, kMixedThreads, kMixedSmem, p->stream>>>(p->d_descs, p->d_items, p->d_count, p->d_counter,
+                                                                     bits);
     MM_CK(cudaGetLastError());
     return MM_OK;
 }
@@ -958,17 +965,20 @@ int mm_b200_plan_create(mm_b200_batch* const* batches, size_t count, size_t quan
     p->grid = std::max(1, per_sm) * dev->sms;
     // Items longest first (by cost per step; every slot of a batch has the same), then by batch
     // and slot.
-    std::vector<std::pair<double, uint2>> items;
+    std::vector<std::pair<double, uint4>> items;
     items.reserve(total);
     for (size_t i = 0; i < count; ++i) {
         const double c = step_cost(batches[i], plan_global(batches[i]));
-        for (size_t s = 0; s < batches[i]->slots; ++s) items.push_back({c, make_uint2((unsigned)i, (unsigned)s)});
+        for (size_t s = 0; s < batches[i]->slots; ++s) items.push_back({c, make_uint4((unsigned)i, (unsigned)s, 0u, 0u)});
     }
     std::stable_sort(items.begin(), items.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
-    std::vector<uint2> it(total);
+    std::vector<uint4> it(total);
     for (size_t i = 0; i < total; ++i) it[i] = items[i].second;
-    MM_CK(cudaMalloc(&p->d_items, total * sizeof(uint2)));
-    MM_CK(cudaMemcpy(p->d_items, it.data(), total * sizeof(uint2), cudaMemcpyHostToDevice));
+    MM_CK(cudaMalloc(&p->d_items, total * sizeof(uint4)));
+    MM_CK(cudaMemcpy(p->d_items, it.data(), total * sizeof(uint4), cudaMemcpyHostToDevice));
+    MM_CK(cudaMalloc(&p->d_count, 2 * sizeof(uint32_t)));
+    const uint32_t counts[2] = {p->count, 0};
+    MM_CK(cudaMemcpy(p->d_count, counts, sizeof(counts), cudaMemcpyHostToDevice));
     MM_CK(cudaMalloc(&p->d_descs, count * sizeof(MixedDesc)));
     MM_CK(cudaMallocHost(&p->h_descs, count * sizeof(MixedDesc)));
     std::memset(p->h_descs, 0, count * sizeof(MixedDesc));
@@ -1086,6 +1096,79 @@ int mm_b200_plan_run_each_async(mm_b200_plan* p, const size_t* steps) {
     return MM_OK;
 }
 
+int mm_b200_plan_run_items(mm_b200_plan* p, size_t count, const uint32_t* batch, const uint32_t* slot,
+                           const uint32_t* steps) {
+    if (!p || (count && (!batch || !slot || !steps))) return fail(MM_ERR_ARG, "plan_run_items: null argument");
+    if (count == 0) return MM_OK;
+    if (count > p->count) return fail(MM_ERR_ARG, "plan_run_items: more items than the plan's slots");
+    MM_CK(cudaSetDevice(p->dev->device));
+    const size_t nb = p->batches.size();
+    // Each slot at most once per launch: two blocks must not step one slot at the same time.
+    std::vector<std::vector<bool>> seen(nb);
+    for (size_t i = 0; i < count; ++i) {
+        if (batch[i] >= nb || slot[i] >= p->batches[batch[i]]->slots)
+            return fail(MM_ERR_ARG, "plan_run_items: bad item " + std::to_string(i));
+        auto& s = seen[batch[i]];
+        if (s.empty()) s.assign(p->batches[batch[i]]->slots, false);
+        if (s[slot[i]]) return fail(MM_ERR_ARG, "plan_run_items: slot listed twice");
+        s[slot[i]] = true;
+    }
+    for (size_t i = 0; i < nb; ++i) {
+        mm_b200_batch* b = p->batches[i];
+        int rc = push(b);
+        if (rc) return rc;
+        MM_CK(cudaEventRecord(p->ready[i], b->stream));
+        MM_CK(cudaStreamWaitEvent(p->stream, p->ready[i], 0));
+    }
+    std::vector<MixedDesc> d(nb);
+    for (size_t i = 0; i < nb; ++i) d[i] = mixed_desc(p->batches[i], plan_global(p->batches[i]), 0);
+    // The pinned list and descriptors may still feed the previous launch's uploads.
+    MM_CK(cudaStreamSynchronize(p->stream));
+    if (std::memcmp(d.data(), p->h_descs, nb * sizeof(MixedDesc)) != 0) {
+        std::memcpy(p->h_descs, d.data(), nb * sizeof(MixedDesc));
+        MM_CK(cudaMemcpyAsync(p->d_descs, p->h_descs, nb * sizeof(MixedDesc), cudaMemcpyHostToDevice, p->stream));
+    }
+    if (!p->d_tick) {
+        MM_CK(cudaMalloc(&p->d_tick, (size_t)p->count * sizeof(uint4)));
+        MM_CK(cudaMallocHost(&p->h_tick, ((size_t)p->count + 1) * sizeof(uint4)));
+        p->tick_cap = p->count;
+    }
+    for (size_t i = 0; i < count; ++i) p->h_tick[i] = make_uint4(batch[i], slot[i], steps[i], 0u);
+    uint32_t* hc = reinterpret_cast<uint32_t*>(p->h_tick + p->tick_cap);
+    hc[0] = (uint32_t)count;
+    MM_CK(cudaMemcpyAsync(p->d_tick, p->h_tick, count * sizeof(uint4), cudaMemcpyHostToDevice, p->stream));
+    MM_CK(cudaMemcpyAsync(p->d_count + 1, hc, 4, cudaMemcpyHostToDevice, p->stream));
+    if (!p->exec_items) {
+        MM_CK(cudaStreamBeginCapture(p->stream, cudaStreamCaptureModeThreadLocal));
+        cudaError_t e0 = cudaMemsetAsync(p->d_counter, 0, 4, p->stream);
+        if (e0 == cudaSuccess)
+            mixed_kernel()<<<p->grid, kMixedThreads, kMixedSmem, p->stream>>>(p->d_descs, p->d_tick, p->d_count + 1,
+                                                                             p->d_counter, 0);
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamEndCapture(p->stream, &g);
+        if (e0 != cudaSuccess) return fail(MM_ERR_CUDA, std::string("plan capture: ") + cudaGetErrorString(e0));
+        if (e != cudaSuccess) return fail(MM_ERR_CUDA, std::string("plan capture: ") + cudaGetErrorString(e));
+        p->graph_items = g;
+        MM_CK(cudaGraphInstantiate(&p->exec_items, p->graph_items, 0));
+    }
+    MM_CK(cudaGraphLaunch(p->exec_items, p->stream));
+    ++p->graph_launches;
+    ++p->launches;
+    for (size_t i = 0; i < count; ++i) {
+        mm_b200_batch* b = p->batches[batch[i]];
+        const size_t s = slot[i];
+        b->pos[s] += std::min<uint32_t>(steps[i], b->nbits[s] - b->pos[s]);
+    }
+    MM_CK(cudaEventRecord(p->done, p->stream));
+    for (auto* b : p->batches) {
+        MM_CK(cudaStreamWaitEvent(b->stream, p->done, 0));
+        b->host_x_valid = false;
+    }
+    return mm_b200_plan_sync(p);
+}
+
+int mm_b200_plan_blocks(const mm_b200_plan* p) { return p ? p->grid : 0; }
+
 int mm_b200_plan_run_each(mm_b200_plan* p, const size_t* steps) {
     int rc = mm_b200_plan_run_each_async(p, steps);
     if (rc) return rc;
@@ -1122,6 +1205,11 @@ void mm_b200_plan_destroy(mm_b200_plan* p) {
     if (p->exec_each) cudaGraphExecDestroy(p->exec_each);
     if (p->graph_each) cudaGraphDestroy(p->graph_each);
     cudaFree(p->d_items);
+    cudaFree(p->d_count);
+    cudaFree(p->d_tick);
+    if (p->h_tick) cudaFreeHost(p->h_tick);
+    if (p->exec_items) cudaGraphExecDestroy(p->exec_items);
+    if (p->graph_items) cudaGraphDestroy(p->graph_items);
     cudaFree(p->d_descs);
     cudaFree(p->d_counter);
     if (p->h_descs) cudaFreeHost(p->h_descs);

@@ -21,8 +21,8 @@ __device__ __noinline__ void mixed_shared(const SlotArgs& a, uint32_t slot, uint
 }
 
 __global__ void __launch_bounds__(kMixedThreads, 2)
-    mixed_step_kernel(const MixedDesc* __restrict__ descs, const uint2* __restrict__ items, uint32_t count,
-                      uint32_t* counter, uint32_t bits) {
+    mixed_step_kernel(const MixedDesc* __restrict__ descs, const uint4* __restrict__ items,
+                      const uint32_t* __restrict__ count_ptr, uint32_t* counter, uint32_t bits) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ uint64_t sc[CarryScratch<kMixedThreads>::words];
     __shared__ uint64_t bars[2];
@@ -30,15 +30,16 @@ __global__ void __launch_bounds__(kMixedThreads, 2)
     const TileSmem sm{smem_raw, bars};
     tile_init(sm);
     uint32_t par = 0;
+    const uint32_t count = *count_ptr;
     for (;;) {
         if (threadIdx.x == 0) next = atomicAdd(counter, 1u);
         __syncthreads();
         const uint32_t i = next;
         __syncthreads();   // every thread has read `next` before thread 0 takes the next item
         if (i >= count) break;
-        const uint2 it = items[i];
+        const uint4 it = items[i];
         const MixedDesc& d = descs[it.x];
-        const uint32_t steps = d.bits ? d.bits : bits;
+        const uint32_t steps = it.z ? it.z : (d.bits ? d.bits : bits);
         if (d.global) {
             if (!gstep_slot<kMixedThreads>(d.g, it.y, steps, sm, sc, par)) break;
             continue;

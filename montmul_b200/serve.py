@@ -5,11 +5,12 @@ Requests arrive as a Poisson process. Each transform length has a lane: uniform 
 ("segments") whose slots keep their Montgomery state and exponent on the device. A request is
 admitted as soon as a slot of its length is free; a lane grows by one segment while the device
 memory budget allows (admission by the per-slot bytes of its length), else the request waits.
-Every tick is one mixed-length plan launch over every busy slot of every lane (persistent blocks
-over a device work queue, replayed from a CUDA graph): the costliest length runs `quantum` steps
-and every other length the steps that take as long (from the tuned cost per step), so no block
-idles while the longest items finish. Then the slots that finished are read back and refilled in
-place with waiting requests: the batch is never drained.
+Every tick is one mixed-length plan launch over a work list of every busy slot (persistent blocks
+over a device work queue, replayed from a CUDA graph). The costliest length runs `quantum` steps
+and every other length the steps that take as long (from the tuned cost per step); when busy
+slots outnumber the resident blocks, the budgets come in two sizes that pack the blocks evenly.
+Then the slots that finished are read back and refilled in place with waiting requests: the
+batch is never drained.
 
 A Fermat request loads 1, sets the exponent N - 1 and reports the verdict x == 1; a mul request
 (a b mod N) takes two slots of the same modulus and one mul launch. Each request's time to
@@ -109,6 +110,7 @@ class Server:
         self.plan_dirty = False
         self.tuned = tuned
         self.steps_done = 0
+        self.gpu_s = 0.0          # wall time inside plan launches (launch, run, wait)
         self.ticks = []           # (t, busy slots, slot-steps run)
         from . import tune
         self.table = tune.load_table().get(dev.device_name(), {})
@@ -210,9 +212,36 @@ class Server:
             # one, so no block idles while the longest items of a tick finish.
             costs = [self.mixed_step_ns(s.batch.params.len) for s in segs]
             top = max(costs)
+            self.seg_ns = costs
             self.seg_steps = [max(1, int(round(self.quantum * top / c))) for c in costs]
+            self.blocks = self.plan.blocks()
             self.plan_dirty = False
         return self.plan
+
+    def work_list(self):
+        """This tick's items (plan batch, slot, steps), longest first. With up to as many busy
+        slots as resident blocks each takes a full budget (the same time for every length). With
+        more, A = q W + r busy slots (0 < r <= W blocks) split into (W - r) q items of 1/q of a
+        budget and r (q + 1) items of 1/(q + 1), so every block ends the tick at once (exactly
+        for q = 1); the slots nearest completion get the larger shares."""
+        items = []
+        for si, seg in enumerate(self.plan_segs):
+            for s in seg.active:
+                rem = seg.batch.remaining(s)
+                items.append([si, s, self.seg_steps[si], rem, self.seg_ns[si]])
+        a, w = len(items), max(1, self.blocks)
+        if a > w:
+            q, r = divmod(a, w)
+            if r == 0:
+                q, r = q - 1, w
+            big = (w - r) * q
+            items.sort(key=lambda it: it[3] * it[4])
+            for i, it in enumerate(items):
+                it[2] = max(1, it[2] // (q if i < big else q + 1))
+        for it in items:
+            it[2] = max(1, min(it[2], it[3]))
+        items.sort(key=lambda it: -it[2] * it[4])
+        return items
 
     def busy(self) -> int:
         return sum(len(s.active) for segs in self.lanes.values() for s in segs)
@@ -220,11 +249,11 @@ class Server:
     def tick(self) -> int:
         """One quantum on every busy slot, then the finished slots are read and freed."""
         plan = self._plan()
-        run = 0
-        for seg, steps in zip(self.plan_segs, self.seg_steps):
-            for s in seg.active:
-                run += min(steps, seg.batch.remaining(s))
-        plan.run_each(self.seg_steps)
+        items = self.work_list()
+        run = sum(it[2] for it in items)
+        t = time.perf_counter()
+        plan.run_items([it[0] for it in items], [it[1] for it in items], [it[2] for it in items])
+        self.gpu_s += time.perf_counter() - t
         now = time.perf_counter() - self.t0
         self.steps_done += run
         self.ticks.append((now, self.busy(), run))
@@ -342,10 +371,10 @@ def summarize(server: Server, reqs, uniform_modsq: float, rate: float, cap: floa
     lat = [r.done - r.arrival for r in ferm]
     end = max(r.done for r in reqs)
     steps = sum(r.n.bit_length() for r in ferm)
-    # Steady window: from the first completion to the last arrival, when the stream is neither
-    # filling nor draining.
-    t_a = min(r.done for r in ferm)
+    # Steady window: the second half of the arrivals, when the stream has filled the GPU and is
+    # not yet draining.
     t_b = max(r.arrival for r in reqs)
+    t_a = t_b / 2
     win = [(t, run) for t, _, run in server.ticks if t_a <= t <= t_b]
     win_modsq = (sum(run for _, run in win) / (win[-1][0] - win[0][0])) if len(win) > 2 else None
     return {
@@ -359,6 +388,8 @@ def summarize(server: Server, reqs, uniform_modsq: float, rate: float, cap: floa
         "p50_s": percentile(lat, 0.5), "p99_s": percentile(lat, 0.99),
         "mul_p50_s": percentile([r.done - r.arrival for r in muls], 0.5) if muls else None,
         "ticks": len(server.ticks), "quantum": server.quantum,
+        "busy_slots_p50": percentile([b for t, b, _ in server.ticks if t_a <= t <= t_b], 0.5),
+        "launch_time_frac": server.gpu_s / end,
         "lanes": {str(L): sum(len(s.batch.moduli) for s in segs) for L, segs in server.lanes.items()},
         "device_bytes": server.used,
     }

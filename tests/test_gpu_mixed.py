@@ -188,3 +188,22 @@ def test_plan_run_each_budgets(dev):
         for i in range(3):
             assert b.remaining(i) == 0 and b.read(i) == powm(base, exps[i], moduli[i])
     assert plan.graph_launches() == 2
+
+
+def test_plan_run_items_lists(dev):
+    """plan.run_items: an explicit work list (any order, per-slot budgets, unlisted slots idle);
+    the same slot twice in one list is rejected."""
+    from montmul_b200.backend import Plan
+    spec = _batches(dev, [4000, 150_000], 3, 40, 29)
+    bs = _arm(dev, spec)
+    plan = Plan(bs, 8)
+    assert plan.blocks() >= 148
+    plan.run_items([1, 0, 0], [2, 0, 1], [30, 5, 40])
+    assert [bs[0].remaining(i) for i in range(3)] == [35, 0, 40]
+    assert [bs[1].remaining(i) for i in range(3)] == [40, 40, 10]
+    with pytest.raises(MontMulError, match="twice"):
+        plan.run_items([0, 0], [2, 2], [1, 1])
+    plan.run_items([0, 0, 1, 1, 1], [0, 2, 0, 1, 2], [35, 40, 40, 40, 10])
+    for (moduli, exps, base), b in zip(spec, bs):
+        for i in range(3):
+            assert b.remaining(i) == 0 and b.read(i) == powm(base, exps[i], moduli[i])

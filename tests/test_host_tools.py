@@ -77,3 +77,51 @@ def test_capacity_and_percentile():
 
 def test_tribonacci_matches_the_reference_sequence():
     assert [tribonacci(i) for i in range(10)] == [0, 0, 1, 1, 2, 4, 7, 13, 24, 44]
+
+
+class _Batch:
+    def __init__(self, rem):
+        self.rem = rem
+
+    def remaining(self, s):
+        return self.rem[s]
+
+
+class _Seg:
+    def __init__(self, rem):
+        self.batch = _Batch(rem)
+        self.active = {s: None for s in rem}
+
+
+def _server(segs, steps, ns, blocks):
+    srv = serve.Server.__new__(serve.Server)
+    srv.plan_segs, srv.seg_steps, srv.seg_ns, srv.blocks = segs, steps, ns, blocks
+    return srv
+
+
+def test_work_list_full_budgets_when_slots_fit():
+    segs = [_Seg({0: 10_000, 1: 50}), _Seg({3: 10_000})]
+    items = _server(segs, [400, 128], [700.0, 2300.0], 8).work_list()
+    assert sorted((b, s, n) for b, s, n, *_ in items) == [(0, 0, 400), (0, 1, 50), (1, 3, 128)]
+    durs = [n * ns for _, _, n, _, ns in items]
+    assert durs == sorted(durs, reverse=True)
+
+
+def test_work_list_packs_blocks_evenly():
+    """A = W + r busy slots on W blocks: W - r full budgets and 2r half budgets, whose work fills
+    every block for one budget's time."""
+    w, a = 10, 14
+    segs = [_Seg({s: 1_000_000 + s for s in range(a)})]
+    items = _server(segs, [100], [1.0], w).work_list()
+    budgets = sorted(n for _, _, n, _, _ in items)
+    assert budgets == [50] * 8 + [100] * 6
+    assert sum(budgets) == w * 100
+    # longest first, so the greedy queue pairs the halves on the remaining blocks
+    assert [n for _, _, n, _, _ in items] == [100] * 6 + [50] * 8
+
+
+def test_work_list_larger_shares_go_to_slots_nearest_completion():
+    segs = [_Seg({0: 5_000, 1: 90_000, 2: 80_000})]
+    items = _server(segs, [1000], [1.0], 2).work_list()
+    got = {s: n for _, s, n, _, _ in items}
+    assert got[0] == 1000 and got[1] == got[2] == 500
