@@ -194,6 +194,8 @@ class Server:
         if not row:
             n = length // 2
             return float(n * max(1, n.bit_length() - 1))
+        if "mixed_ns" in row:
+            return row["mixed_ns"]
         if length > 8192:
             g = [c["step_ns"] for c in row.get("candidates", []) if c["global"]]
             if g:

@@ -9,8 +9,9 @@ the device and keeps the fastest:
   - steps per launch (launch_steps): a longer launch saves launch gaps, a shorter one bounds how
     long a batch holds the GPU.
 
-It records the winner's time per slot-step (step_ns), which also orders the work items of a
-mixed-length launch. The fixed parts of a schedule are reported beside it: threads per block,
+It records the winner's time per slot-step (step_ns), and the length's time per slot-step inside
+the mixed-length persistent launch (mixed_ns), which orders that launch's work items and sizes a
+serving tick's budgets. The fixed parts of a schedule are reported beside it: threads per block,
 the radix schedule of the length-n transform, the tile length of global mode and the blocks per
 SM. The table is JSON keyed by device name, cached at $MONTMUL_B200_SCHEDULES or
 ~/.cache/montmul_b200/schedules.json; without a cache the table shipped in the package
@@ -31,6 +32,7 @@ TILE = 2048           # global mode's tile length (elements of n)
 MAX_SHARED_N = 8192   # n <= 8192 fits the shared-memory kernels
 MIN_GLOBAL_N = 4096   # global mode from n = 4096 (L = 8192)
 LAUNCH_STEPS = (64, 512)
+MAX_MIXED_L = 65536     # lengths whose cost inside the mixed launch is measured too
 
 
 # The table measured on a B200 and shipped with the package; used when no cache exists.
@@ -107,6 +109,29 @@ def measure(dev, length: int, global_mode: bool, launch_steps: int, slots: int, 
     return dt / (slots * steps)
 
 
+def measure_mixed(dev, length: int, slots: int, steps: int, seed: int = 2026):
+    """Seconds per slot-step of one length inside the mixed-length persistent launch (256-thread
+    blocks, two per SM; global mode above L = 8192), at full occupancy: the cost that orders a
+    mixed launch's items and sizes a serving tick's budgets."""
+    from .backend import Plan
+    from .batch import ModBatch
+    from .gmp import RandState
+    rng = RandState(seed)
+    bits = bits_for(length)
+    moduli = [rng.random_bits(bits) | (1 << (bits - 1)) | 1 for _ in range(slots)]
+    exps = [rng.random_bits(steps + 8) | (1 << (steps + 7)) for _ in range(slots)]
+    b = ModBatch(dev, moduli, 3)
+    b.load_all([1] * slots)
+    b.set_exponents(exps)
+    plan = Plan([b], steps + 8)
+    plan.run(8)
+    t = time.perf_counter()
+    plan.run(steps)
+    dt = time.perf_counter() - t
+    plan.close()
+    return dt / (slots * steps)
+
+
 def tune_length(dev, length: int, budget_s: float = 4.0):
     """The fastest schedule of one length, with every candidate's time."""
     sms = dev.sm_count()
@@ -126,6 +151,8 @@ def tune_length(dev, length: int, budget_s: float = 4.0):
     out["slots"] = slots
     out["steps"] = steps
     out["candidates"] = results
+    if length <= MAX_MIXED_L:
+        out["mixed_ns"] = measure_mixed(dev, length, slots, max(8, min(steps, 1000))) * 1e9
     return out
 
 
@@ -161,7 +188,7 @@ def apply(batch, table=None) -> bool:
     sc = schedule_for(be.device_name(), batch.params.len, table)
     if not sc:
         return False
-    be.set_schedule(st, sc["global"], sc["launch_steps"], sc["step_ns"])
+    be.set_schedule(st, sc["global"], sc["launch_steps"], sc.get("mixed_ns", sc["step_ns"]))
     return True
 
 
@@ -170,7 +197,13 @@ def tune(dev, lengths, force: bool = False, log=print):
     name = dev.device_name()
     per = table.setdefault(name, {})
     for length in lengths:
-        if str(length) in per and not force:
+        row = per.get(str(length))
+        if row and not force:
+            if "mixed_ns" not in row and length <= MAX_MIXED_L:
+                steps = max(8, min(int(row.get("steps", 64)), 1000))
+                row["mixed_ns"] = measure_mixed(dev, length, int(row.get("slots", 8 * dev.sm_count())), steps) * 1e9
+                log(f"L={length}: {row['mixed_ns'] / 1e3:.2f} us/slot-step in the mixed launch")
+                save_table(table)
             continue
         r = tune_length(dev, length)
         per[str(length)] = r
