@@ -182,10 +182,13 @@ int mm_b200_read_slots(mm_b200_batch *b, size_t count, const size_t *slots, uint
 /* ---- Mixed-length persistent launch (no counterpart in the reference) ----
  * A plan covers every slot of `count` batches on one device, of any lengths. plan_run runs up
  * to `bits` steps on every slot with bits left, like run on each batch, but in persistent
- * launches of 256-thread blocks (two per SM) that take (batch, slot) items from a device work
- * queue, longest first; each launch covers `quantum` steps and is replayed from a CUDA graph.
- * Batches of L <= 8192 run with the vector in shared memory, longer ones in global mode. The
- * batches must outlive the plan; plan_sync performs run's error check on every batch. */
+ * launches (one 512-thread block per SM) that take (batch, slot) items from device work queues;
+ * each launch covers `quantum` steps and is replayed from a CUDA graph. A block first takes
+ * "wide" items (L = 16384 batches in shared mode: the whole block and all its shared memory on
+ * one slot), then splits into two 256-thread workers that take the other items longest first:
+ * L <= 8192 with the vector in shared memory, longer lengths and batches tuned to global mode in
+ * global mode. The batches must outlive the plan; plan_sync performs run's error check on every
+ * batch. */
 typedef struct mm_b200_plan mm_b200_plan;
 int mm_b200_plan_create(mm_b200_batch *const *batches, size_t count, size_t quantum, mm_b200_plan **out);
 int mm_b200_plan_run_async(mm_b200_plan *p, size_t bits);
@@ -197,12 +200,17 @@ int mm_b200_plan_run(mm_b200_plan *p, size_t bits);
 int mm_b200_plan_run_each_async(mm_b200_plan *p, const size_t *steps);
 int mm_b200_plan_run_each(mm_b200_plan *p, const size_t *steps);
 /* One launch over an explicit work list, taken in list order: item i runs up to steps[i]
- * (>= 1) steps of slot slot[i] of batch batch[i]; each slot at most once. A scheduler orders the
- * list longest first and sizes the budgets so the plan's resident blocks (plan_blocks) finish
- * together. Waits for the launch and checks errors, as plan_run. */
+ * (>= 1) steps of slot slot[i] of batch batch[i]; each slot at most once. The wide items of the
+ * list run first, then the others, each kind in list order. A scheduler orders the list longest
+ * first and sizes the budgets so the plan's workers finish together. Waits for the launch and
+ * checks errors, as plan_run. */
 int mm_b200_plan_run_items(mm_b200_plan *p, size_t count, const uint32_t *batch, const uint32_t *slot,
                            const uint32_t *steps);
+/* Workers of the plan's launch that take items other than wide ones (two per block), the
+ * blocks (each takes wide items one at a time), and whether batch i's items are wide. */
 int mm_b200_plan_blocks(const mm_b200_plan *p);
+int mm_b200_plan_wide_blocks(const mm_b200_plan *p);
+int mm_b200_plan_batch_wide(const mm_b200_plan *p, size_t i);
 void *mm_b200_plan_stream(mm_b200_plan *p);
 /* Kernel launches of the plan so far, and how many of them were graph replays. */
 uint64_t mm_b200_plan_launches(const mm_b200_plan *p);

@@ -6,7 +6,7 @@
     python -m montmul_b200 sweep [--bits 1024 8192 ...] [--slots S] [--ebits 256]
     python -m montmul_b200 mixed [--slots 2000] [--lo 8192] [--hi 300000] [--ebits 1000]
     python -m montmul_b200 serve [--load 0.7 0.95] [--duration 40] [--lo 10000] [--hi 200000]
-    python -m montmul_b200 tune  [--lengths ...] [--force]
+    python -m montmul_b200 tune  [--lengths ...] [--force] [--mixed-only]
 
 bench, prp and score print `key=value` fields as the reference does (and append a CSV row with
 --csv); sweep, mixed and serve print one JSON object. Only the b200 backend is part of this
@@ -156,6 +156,7 @@ def main(argv=None) -> int:
     p = sub.add_parser("tune", allow_abbrev=False)
     p.add_argument("--lengths", type=int, nargs="*", default=[1 << e for e in range(8, 18)])
     p.add_argument("--force", action="store_true")
+    p.add_argument("--mixed-only", action="store_true")
     for p in sub.choices.values():
         p.add_argument("--device", type=int, default=0)
     args = sys.argv[1:] if argv is None else list(argv)
@@ -187,7 +188,8 @@ def main(argv=None) -> int:
         return 0
     if a.cmd == "tune":
         from . import tune
-        return tune.main(["--lengths", *map(str, a.lengths), "--device", str(a.device)] + (["--force"] if a.force else []))
+        return tune.main(["--lengths", *map(str, a.lengths), "--device", str(a.device)] + (["--force"] if a.force else [])
+                         + (["--mixed-only"] if a.mixed_only else []))
     return 2
 
 

@@ -75,6 +75,8 @@ SIGNATURES = {
     "mm_b200_plan_run_each": ([_vp, _vp], C.c_int),
     "mm_b200_plan_run_items": ([_vp, _sz, _vp, _vp, _vp], C.c_int),
     "mm_b200_plan_blocks": ([_vp], C.c_int),
+    "mm_b200_plan_wide_blocks": ([_vp], C.c_int),
+    "mm_b200_plan_batch_wide": ([_vp, _sz], C.c_int),
     "mm_b200_plan_run": ([_vp, _sz], C.c_int),
     "mm_b200_plan_stream": ([_vp], _vp),
     "mm_b200_plan_launches": ([_vp], C.c_uint64),
@@ -393,8 +395,18 @@ class Plan:
         _check(lib().mm_b200_plan_run_items(self._p, b.size, _ptr(b), _ptr(s), _ptr(t)))
 
     def blocks(self) -> int:
-        """Resident blocks of the plan's launch (items that run at once)."""
+        """Workers of the plan's launch that take items other than wide ones (items that run
+        at once; two per block)."""
         return int(lib().mm_b200_plan_blocks(self._p))
+
+    def wide_blocks(self) -> int:
+        """Blocks of the plan's launch; each takes wide items (L = 16384 in shared mode) one
+        at a time, before its two workers take the other items."""
+        return int(lib().mm_b200_plan_wide_blocks(self._p))
+
+    def batch_wide(self, i: int) -> bool:
+        """Whether the slots of batch i run as wide items."""
+        return bool(lib().mm_b200_plan_batch_wide(self._p, i))
 
     def run_each(self, steps) -> None:
         """One launch in which the slots of batch i run up to steps[i] steps."""

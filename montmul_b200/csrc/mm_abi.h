@@ -62,18 +62,35 @@ constexpr int kMinGlobalLogN = 12;   // smallest length the global kernels accep
 GlobalKernels global_kernels();       // mm_global.cu
 
 // The mixed-length persistent launch (mm_mixed.cu): one descriptor per batch, one work item
-// (descriptor index, slot) per slot; blocks take items from a device counter in item order.
+// (descriptor index, slot) per slot. Each block first takes "wide" items (L = 16384 in shared
+// mode, the whole block on one slot with the vector in all of its shared memory), then splits
+// into groups of kMixedThreads threads that take the other items, each group with its own
+// 96 KiB of shared memory; both lists are taken from device counters in list order.
 struct MixedDesc {
     GArgs g;        // the batch's slot state (w2 / w1 unused in shared mode)
-    int global;     // 1: global mode; 0: the vector in shared memory (m <= kMaxMixedSharedLogN)
+    int global;     // 1: global mode; 0: the vector in shared memory
     uint32_t bits;  // steps per item of this batch in this launch (0: the launch's `bits`)
 };
-constexpr int kMixedThreads = 256;
-constexpr int kMaxMixedSharedLogN = 12;   // 96 KiB: two blocks per SM, as global mode
-constexpr int kMixedSmem = 24 << kMaxMixedSharedLogN;
+constexpr int kMixedThreads = 256;        // one group: the threads on one slot
+constexpr int kMixedGroups = 2;           // groups per block
+constexpr int kMixedBlockThreads = kMixedThreads * kMixedGroups;
+constexpr int kMaxMixedSharedLogN = 12;   // 96 KiB per group, as global mode's tiles
+constexpr int kMixedGroupSmem = 24 << kMaxMixedSharedLogN;
+constexpr int kMixedSmem = kMixedGroups * kMixedGroupSmem;
+constexpr int kWideLogN = kMaxSharedLogN;  // n = 8192: 24 n bytes = all of a block's shared memory
+constexpr int kWideThreads = kMixedBlockThreads;
+static_assert(kMixedSmem == (24 << kWideLogN), "one wide vector fills the groups' shared memory");
 // Items: (descriptor, slot, steps, unused); steps 0 takes the descriptor's, then the launch's.
-// The item count is read from device memory, so one captured launch serves any list.
-typedef void (*MixedFn)(const MixedDesc*, const uint4*, const uint32_t*, uint32_t*, uint32_t);
+// The item counts are read from device memory, so one captured launch serves any lists.
+// counter[0] counts the group items taken, counter[1] the wide items.
+struct MixedLists {
+    const uint4* items;
+    const uint32_t* count;
+    const uint4* wide;
+    const uint32_t* wide_count;
+    uint32_t* counter;
+};
+typedef void (*MixedFn)(const MixedDesc*, MixedLists, uint32_t);
 MixedFn mixed_kernel();               // mm_mixed.cu
 
 // Threads per block for transform length 2^m: one radix-8 group per thread up to 256 threads.

@@ -92,7 +92,7 @@ struct mm_b200_batch {
     GlobalKernels gk{};
     F2* d_w2 = nullptr;        // global mode: slots x n work elements
     F1* d_w1 = nullptr;
-    const DevTables* gtab = nullptr;   // global-mode tables (global batches; L = 16384 in a mixed plan)
+    const DevTables* gtab = nullptr;   // global-mode tables (global batches)
     mm_b200_schedule sched{0, 0, 0.0};
     uint32_t* d_stage = nullptr;       // refill staging: device words and pinned host words
     size_t stage_cap = 0;
@@ -292,8 +292,7 @@ int launch_steps(mm_b200_batch* b, size_t bits, bool bare = false) {
     return MM_OK;
 }
 
-// Global-mode work vectors and tables for a batch created in shared mode (a schedule switch, or
-// L = 16384 in a mixed plan, whose blocks have 96 KiB of shared memory).
+// Global-mode work vectors and tables for a batch created in shared mode (a schedule switch).
 int ensure_global_buffers(mm_b200_batch* b) {
     if (b->m < kMinGlobalLogN) return fail(MM_ERR_UNSUPPORTED, "global mode needs L >= 8192");
     if (!b->gtab) {
@@ -869,12 +868,14 @@ struct mm_b200_plan {
     int grid = 0;
     MixedDesc* d_descs = nullptr;
     MixedDesc* h_descs = nullptr;     // pinned copy of what the device holds
-    uint4* d_items = nullptr;          // every slot, longest first (plan_run, plan_run_each)
-    uint32_t count = 0;
-    uint32_t* d_count = nullptr;       // [0]: count of d_items; [1]: count of the tick list
-    uint4* d_tick = nullptr;           // plan_run_items' list
-    uint4* h_tick = nullptr;           // pinned staging of that list (+ its count)
-    size_t tick_cap = 0;
+    // Every slot (plan_run, plan_run_each): the group items longest first, then the wide items.
+    uint4* d_items = nullptr;
+    uint4* d_wide = nullptr;
+    uint32_t count = 0;                // slots of all batches
+    // [0], [1]: counts of d_items and d_wide; [2], [3]: counts of plan_run_items' two lists.
+    uint32_t* d_count = nullptr;
+    uint4* d_tick = nullptr;           // plan_run_items' lists: group items at 0, wide at `count`
+    uint4* h_tick = nullptr;           // pinned staging of those lists (+ their counts)
     cudaGraph_t graph_items = nullptr;
     cudaGraphExec_t exec_items = nullptr;
     uint32_t* d_counter = nullptr;
@@ -909,14 +910,24 @@ MixedDesc mixed_desc(const mm_b200_batch* b, bool global, uint32_t bits) {
     return d;
 }
 
-bool plan_global(const mm_b200_batch* b) { return b->global || b->m > kMaxMixedSharedLogN; }
+// A batch whose slots run as wide items (a whole block each, the vector in shared memory).
+bool plan_wide(const mm_b200_batch* b) { return !b->global && b->m == kWideLogN; }
+// A batch whose slots run in global mode inside the mixed launch.
+bool plan_global(const mm_b200_batch* b) { return b->global || b->m > kWideLogN; }
 
-// One launch of `bits` steps: the counter reset and the persistent kernel.
+// The counter reset and one persistent launch over lists `items` (count at count[0]) and `wide`
+// (count at count[1]).
+cudaError_t plan_launch(mm_b200_plan* p, const uint4* items, const uint4* wide, const uint32_t* count, uint32_t bits) {
+    cudaError_t e = cudaMemsetAsync(p->d_counter, 0, 2 * sizeof(uint32_t), p->stream);
+    if (e != cudaSuccess) return e;
+    const MixedLists l{items, count, wide, count + 1, p->d_counter};
+    mixed_kernel()<<<p->grid, kMixedBlockThreads, kMixedSmem, p->stream>>>(p->d_descs, l, bits);
+    return cudaGetLastError();
+}
+
+// One launch of `bits` steps over every slot.
 int plan_enqueue(mm_b200_plan* p, uint32_t bits) {
-    MM_CK(cudaMemsetAsync(p->d_counter, 0, 4, p->stream));
-    mixed_kernel()<<<p->grid, kMixedThreads, kMixedSmem, p->stream>>>(p->d_descs, p->d_items, p->d_count, p->d_counter,
-                                                                     bits);
-    MM_CK(cudaGetLastError());
+    MM_CK(plan_launch(p, p->d_items, p->d_wide, p->d_count, bits));
     return MM_OK;
 }
 
@@ -961,28 +972,36 @@ int mm_b200_plan_create(mm_b200_batch* const* batches, size_t count, size_t quan
         }
     }
     int per_sm = 0;
-    MM_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, mixed_kernel(), kMixedThreads, kMixedSmem));
-    p->grid = std::max(1, per_sm) * dev->sms;
-    // Items longest first (by cost per step; every slot of a batch has the same), then by batch
-    // and slot.
+    MM_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, mixed_kernel(), kMixedBlockThreads, kMixedSmem));
+    if (per_sm < 1) return fail(MM_ERR_CUDA, "plan_create: the mixed launch fits no block on an SM");
+    p->grid = per_sm * dev->sms;
+    // Group items longest first (by cost per step; every slot of a batch has the same), then by
+    // batch and slot; wide items by batch and slot.
     std::vector<std::pair<double, uint4>> items;
+    std::vector<uint4> wide;
     items.reserve(total);
     for (size_t i = 0; i < count; ++i) {
         const double c = step_cost(batches[i], plan_global(batches[i]));
-        for (size_t s = 0; s < batches[i]->slots; ++s) items.push_back({c, make_uint4((unsigned)i, (unsigned)s, 0u, 0u)});
+        for (size_t s = 0; s < batches[i]->slots; ++s) {
+            const uint4 it = make_uint4((unsigned)i, (unsigned)s, 0u, 0u);
+            if (plan_wide(batches[i])) wide.push_back(it);
+            else items.push_back({c, it});
+        }
     }
     std::stable_sort(items.begin(), items.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
     std::vector<uint4> it(total);
-    for (size_t i = 0; i < total; ++i) it[i] = items[i].second;
+    for (size_t i = 0; i < items.size(); ++i) it[i] = items[i].second;
+    std::copy(wide.begin(), wide.end(), it.begin() + items.size());
     MM_CK(cudaMalloc(&p->d_items, total * sizeof(uint4)));
     MM_CK(cudaMemcpy(p->d_items, it.data(), total * sizeof(uint4), cudaMemcpyHostToDevice));
-    MM_CK(cudaMalloc(&p->d_count, 2 * sizeof(uint32_t)));
-    const uint32_t counts[2] = {p->count, 0};
+    p->d_wide = p->d_items + items.size();
+    MM_CK(cudaMalloc(&p->d_count, 4 * sizeof(uint32_t)));
+    const uint32_t counts[4] = {(uint32_t)items.size(), (uint32_t)wide.size(), 0, 0};
     MM_CK(cudaMemcpy(p->d_count, counts, sizeof(counts), cudaMemcpyHostToDevice));
     MM_CK(cudaMalloc(&p->d_descs, count * sizeof(MixedDesc)));
     MM_CK(cudaMallocHost(&p->h_descs, count * sizeof(MixedDesc)));
     std::memset(p->h_descs, 0, count * sizeof(MixedDesc));
-    MM_CK(cudaMalloc(&p->d_counter, 4));
+    MM_CK(cudaMalloc(&p->d_counter, 2 * sizeof(uint32_t)));
     *out = p.release();
     return MM_OK;
 }
@@ -1128,22 +1147,28 @@ int mm_b200_plan_run_items(mm_b200_plan* p, size_t count, const uint32_t* batch,
         std::memcpy(p->h_descs, d.data(), nb * sizeof(MixedDesc));
         MM_CK(cudaMemcpyAsync(p->d_descs, p->h_descs, nb * sizeof(MixedDesc), cudaMemcpyHostToDevice, p->stream));
     }
+    const size_t cap = p->count;
     if (!p->d_tick) {
-        MM_CK(cudaMalloc(&p->d_tick, (size_t)p->count * sizeof(uint4)));
-        MM_CK(cudaMallocHost(&p->h_tick, ((size_t)p->count + 1) * sizeof(uint4)));
-        p->tick_cap = p->count;
+        MM_CK(cudaMalloc(&p->d_tick, 2 * cap * sizeof(uint4)));
+        MM_CK(cudaMallocHost(&p->h_tick, (2 * cap + 1) * sizeof(uint4)));
     }
-    for (size_t i = 0; i < count; ++i) p->h_tick[i] = make_uint4(batch[i], slot[i], steps[i], 0u);
-    uint32_t* hc = reinterpret_cast<uint32_t*>(p->h_tick + p->tick_cap);
-    hc[0] = (uint32_t)count;
-    MM_CK(cudaMemcpyAsync(p->d_tick, p->h_tick, count * sizeof(uint4), cudaMemcpyHostToDevice, p->stream));
-    MM_CK(cudaMemcpyAsync(p->d_count + 1, hc, 4, cudaMemcpyHostToDevice, p->stream));
+    // The list splits into group items (in list order) at 0 and wide items (in list order) at cap.
+    size_t ng = 0, nw = 0;
+    for (size_t i = 0; i < count; ++i) {
+        const uint4 it = make_uint4(batch[i], slot[i], steps[i], 0u);
+        if (plan_wide(p->batches[batch[i]])) p->h_tick[cap + nw++] = it;
+        else p->h_tick[ng++] = it;
+    }
+    uint32_t* hc = reinterpret_cast<uint32_t*>(p->h_tick + 2 * cap);
+    hc[0] = (uint32_t)ng;
+    hc[1] = (uint32_t)nw;
+    if (ng) MM_CK(cudaMemcpyAsync(p->d_tick, p->h_tick, ng * sizeof(uint4), cudaMemcpyHostToDevice, p->stream));
+    if (nw)
+        MM_CK(cudaMemcpyAsync(p->d_tick + cap, p->h_tick + cap, nw * sizeof(uint4), cudaMemcpyHostToDevice, p->stream));
+    MM_CK(cudaMemcpyAsync(p->d_count + 2, hc, 2 * sizeof(uint32_t), cudaMemcpyHostToDevice, p->stream));
     if (!p->exec_items) {
         MM_CK(cudaStreamBeginCapture(p->stream, cudaStreamCaptureModeThreadLocal));
-        cudaError_t e0 = cudaMemsetAsync(p->d_counter, 0, 4, p->stream);
-        if (e0 == cudaSuccess)
-            mixed_kernel()<<<p->grid, kMixedThreads, kMixedSmem, p->stream>>>(p->d_descs, p->d_tick, p->d_count + 1,
-                                                                             p->d_counter, 0);
+        const cudaError_t e0 = plan_launch(p, p->d_tick, p->d_tick + cap, p->d_count + 2, 0);
         cudaGraph_t g = nullptr;
         cudaError_t e = cudaStreamEndCapture(p->stream, &g);
         if (e0 != cudaSuccess) return fail(MM_ERR_CUDA, std::string("plan capture: ") + cudaGetErrorString(e0));
@@ -1167,7 +1192,13 @@ int mm_b200_plan_run_items(mm_b200_plan* p, size_t count, const uint32_t* batch,
     return mm_b200_plan_sync(p);
 }
 
-int mm_b200_plan_blocks(const mm_b200_plan* p) { return p ? p->grid : 0; }
+int mm_b200_plan_blocks(const mm_b200_plan* p) { return p ? p->grid * kMixedGroups : 0; }
+
+int mm_b200_plan_wide_blocks(const mm_b200_plan* p) { return p ? p->grid : 0; }
+
+int mm_b200_plan_batch_wide(const mm_b200_plan* p, size_t i) {
+    return p && i < p->batches.size() && plan_wide(p->batches[i]) ? 1 : 0;
+}
 
 int mm_b200_plan_run_each(mm_b200_plan* p, const size_t* steps) {
     int rc = mm_b200_plan_run_each_async(p, steps);

@@ -25,11 +25,11 @@ template <int E, int TA, int NT>
 __device__ __forceinline__ uint64_t block_resolve(uint32_t (&L)[E], uint64_t c, uint64_t cin0, uint64_t* sc) {
     static_assert(E >= 2, "a segment must hold at least 64 bits");
     constexpr int W = (NT + 31) / 32;
-    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    const int t = gtid<NT>(), lane = t & 31, w = t >> 5;
     const bool act = t < TA;
     if (lane == 31) sc[w] = c;
     if (t == TA - 1) sc[W] = c;
-    __syncthreads();
+    gsync<NT>();
     const uint64_t up = __shfl_up_sync(0xffffffffu, c, 1);
     const uint64_t cin = (t == 0) ? cin0 : (lane == 0 ? sc[w - 1] : up);
     uint32_t r = 0;
@@ -52,7 +52,7 @@ __device__ __forceinline__ uint64_t block_resolve(uint32_t (&L)[E], uint64_t c, 
     const uint32_t wprop = (Y == 0xffffffffu) && !wgen;
     uint64_t* summ = sc + W + 1;
     if (lane == 0) summ[w] = wgen | (wprop << 1);
-    __syncthreads();
+    gsync<NT>();
     const uint64_t f = lane < W ? summ[lane] : 0;
     const uint32_t gw = __ballot_sync(0xffffffffu, f & 1);
     const uint32_t yw = gw | __ballot_sync(0xffffffffu, (f >> 1) & 1);
@@ -69,7 +69,7 @@ __device__ __forceinline__ uint64_t block_resolve(uint32_t (&L)[E], uint64_t c, 
         }
     }
     const uint64_t top = sc[W] + ((sw >> W) & 1);
-    __syncthreads();
+    gsync<NT>();
     return top;
 }
 
@@ -94,7 +94,7 @@ template <int M, int NT>
 __device__ __noinline__ uint64_t carry_product(const F2* s2, const F1* s1, uint32_t* __restrict__ out, uint64_t* sc) {
     constexpr int N = 1 << M, COUNT = 2 * N;
     constexpr int E = cmax(2, COUNT / NT), TA = COUNT / E;
-    const int t = threadIdx.x;
+    const int t = gtid<NT>();
     uint32_t L[E];
     uint64_t c = 0;
     const int q0 = t * E;
@@ -120,7 +120,7 @@ __device__ __noinline__ uint64_t carry_product(const F2* s2, const F1* s1, uint3
 #pragma unroll
         for (int e = 0; e < E; ++e) out[q0 + e] = L[e];
     }
-    __syncthreads();
+    gsync<NT>();
     return top;
 }
 
@@ -130,7 +130,7 @@ template <int M, int NT>
 __device__ __noinline__ void carry_low_and_pack(F2* s2, F1* s1, uint64_t* sc) {
     constexpr int N = 1 << M, COUNT = N;
     constexpr int E = cmax(2, COUNT / NT), TA = COUNT / E;
-    const int t = threadIdx.x;
+    const int t = gtid<NT>();
     uint32_t L[E];
     uint64_t c = 0;
     const int q0 = t * E;
@@ -159,7 +159,7 @@ __device__ __noinline__ void carry_low_and_pack(F2* s2, F1* s1, uint64_t* sc) {
             s1[swz(j)] = z1;
         }
     }
-    __syncthreads();
+    gsync<NT>();
 }
 
 // m = the low k limbs of a product whose low n coefficients are the real parts of the first n
@@ -169,7 +169,7 @@ template <int M, int NT>
 __device__ __noinline__ void carry_low_to(const F2* s2, const F1* s1, uint32_t* __restrict__ out, int k, uint64_t* sc) {
     constexpr int N = 1 << M, COUNT = N;
     constexpr int E = cmax(2, COUNT / NT), TA = COUNT / E;
-    const int t = threadIdx.x;
+    const int t = gtid<NT>();
     uint32_t L[E];
     uint64_t c = 0;
     const int q0 = t * E;
@@ -192,7 +192,7 @@ __device__ __noinline__ void carry_low_to(const F2* s2, const F1* s1, uint32_t* 
         for (int e = 0; e < E; ++e)
             if (q0 + e < k) out[q0 + e] = L[e];
     }
-    __syncthreads();
+    gsync<NT>();
 }
 
 // x = (T + m N) / R without the wraparound path (cpu.rs:470-481): the product m N in natural
@@ -204,7 +204,7 @@ __device__ __noinline__ bool carry_shift_add(const F2* s2, const F1* s1, const u
                                              uint32_t* __restrict__ x, int k, uint32_t flag, uint64_t* sc) {
     constexpr int N = 1 << M, COUNT = 2 * N;
     constexpr int E = cmax(2, COUNT / NT), TA = COUNT / E;
-    const int t = threadIdx.x;
+    const int t = gtid<NT>();
     uint32_t L[E];
     uint64_t c = 0;
     const int q0 = t * E;
@@ -239,7 +239,7 @@ __device__ __noinline__ bool carry_shift_add(const F2* s2, const F1* s1, const u
             else if (q >= 2 * k) stray |= L[e] != 0;
         }
     }
-    return !__syncthreads_or(stray) && top == 0;
+    return !gsync_or<NT>(stray) && top == 0;
 }
 
 // x = floor(T / R) + ((cyclic + T mod R) mod (R - 1)) with the cyclic product m N mod (R - 1)
@@ -251,7 +251,7 @@ __device__ __noinline__ bool wrap_combine(const F2* s2, const F1* s1, const uint
                                              uint32_t* __restrict__ x, uint64_t* sc) {
     constexpr int K = 1 << M, COUNT = K;
     constexpr int E = cmax(2, COUNT / NT), TA = COUNT / E;
-    const int t = threadIdx.x;
+    const int t = gtid<NT>();
     uint32_t L[E];
     uint64_t c = 0;
     const int q0 = t * E;
@@ -296,7 +296,7 @@ __device__ __noinline__ bool wrap_combine(const F2* s2, const F1* s1, const uint
 #pragma unroll
         for (int e = 0; e < E; ++e) x[q0 + e] = L[e];
     }
-    __syncthreads();
+    gsync<NT>();
     return top == 0;
 }
 

@@ -126,7 +126,7 @@ __device__ __noinline__ void g_dif_first(const uint32_t* __restrict__ lim, int c
                                          const F1* t1, const F2K* cin2, const F1* cin1, int lq) {
     const int q = 1 << lq;
 #pragma unroll 1
-    for (int j = threadIdx.x; j < q; j += NT) {
+    for (int j = gtid<NT>(); j < q; j += NT) {
         uint32_t v[R];
 #pragma unroll
         for (int k = 0; k < R; ++k) v[k] = (j + k * q < cnt) ? lim[j + k * q] : 0u;
@@ -147,7 +147,7 @@ __device__ __noinline__ void g_dif_first(const uint32_t* __restrict__ lim, int c
             for (int k = 0; k < R; ++k) v1[swz(j + k * q)] = cmul(x[k], t1[k * q + j]);
         }
     }
-    __syncthreads();
+    gsync<NT>();
 }
 
 // Weighted last global DIT pass into natural order (runtime span), as dit_last_weighted.
@@ -156,7 +156,7 @@ __device__ __noinline__ void g_dit_last(F2* v2, F1* v1, const F2K* t2, const F1*
                                         const F1* cout1, int lq) {
     const int q = 1 << lq;
 #pragma unroll 1
-    for (int j = threadIdx.x; j < q; j += NT) {
+    for (int j = gtid<NT>(); j < q; j += NT) {
         {
             F2 x[R];
 #pragma unroll
@@ -180,7 +180,7 @@ __device__ __noinline__ void g_dit_last(F2* v2, F1* v1, const F2K* t2, const F1*
             }
         }
     }
-    __syncthreads();
+    gsync<NT>();
 }
 
 // Weighted first global pass of complex elements in place (the Transform trait's forward, as
@@ -190,7 +190,7 @@ __device__ __noinline__ void g_dif_first_complex(F2* v2, F1* v1, const F2K* t2, 
                                                  const F1* cin1, int lq) {
     const int q = 1 << lq;
 #pragma unroll 1
-    for (int j = threadIdx.x; j < q; j += NT) {
+    for (int j = gtid<NT>(); j < q; j += NT) {
         {
             F2 x[R];
 #pragma unroll
@@ -208,7 +208,7 @@ __device__ __noinline__ void g_dif_first_complex(F2* v2, F1* v1, const F2K* t2, 
             for (int k = 0; k < R; ++k) v1[swz(j + k * q)] = cmul(x[k], t1[k * q + j]);
         }
     }
-    __syncthreads();
+    gsync<NT>();
 }
 
 template <int NT>
@@ -263,14 +263,15 @@ struct TileSmem {
     __device__ F1* b1(int b) const { return reinterpret_cast<F1*>(base + b * (kTileBytes2 + kTileBytes1) + kTileBytes2); }
 };
 
-// Once per kernel, all threads.
+// Once per kernel, all threads of the group.
+template <int NT>
 __device__ __forceinline__ void tile_init(const TileSmem& sm) {
-    if (threadIdx.x == 0) {
+    if (gtid<NT>() == 0) {
         mbar_init(&sm.bar[0]);
         mbar_init(&sm.bar[1]);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    __syncthreads();
+    gsync<NT>();
 }
 
 // The mbarrier phases: bit b of `par` is the parity of the next phase of barrier b. Tile c uses
@@ -291,10 +292,13 @@ __device__ __noinline__ bool tile_phase(F2* v2, F1* v1, int n, const F2K* tt2, c
     const int tiles = n >> kTileLog;
     const bool store = mode != kTileDifOp;
     constexpr uint32_t kBytes = kTileBytes2 + kTileBytes1;
-    // This thread's generic writes of the vector (earlier passes) before the bulk loads read it.
+    // This thread's generic writes of the vector (earlier passes) before the bulk loads read it,
+    // and its generic accesses of the tile buffers (a shared-mode item of the mixed launch may
+    // have used them) before the bulk loads overwrite them.
     fence_async_global();
-    __syncthreads();
-    if (threadIdx.x == 0) {
+    fence_async_shared();
+    gsync<NT>();
+    if (gtid<NT>() == 0) {
         mbar_expect(&sm.bar[0], kBytes);
         bulk_load(sm.b2(0), v2, kTileBytes2, &sm.bar[0]);
         bulk_load(sm.b1(0), v1, kTileBytes1, &sm.bar[0]);
@@ -304,7 +308,7 @@ __device__ __noinline__ bool tile_phase(F2* v2, F1* v1, int n, const F2K* tt2, c
     for (int c = 0; c < tiles; ++c) {
         const int b = c & 1;
         const uint32_t ph = ((par >> b) ^ (uint32_t)(c >> 1)) & 1;
-        if (threadIdx.x == 0 && c + 1 < tiles) {
+        if (gtid<NT>() == 0 && c + 1 < tiles) {
             // The other buffer's store (tile c - 1) must have read its data out first.
             bulk_wait_read();
             mbar_expect(&sm.bar[b ^ 1], kBytes);
@@ -312,9 +316,9 @@ __device__ __noinline__ bool tile_phase(F2* v2, F1* v1, int n, const F2K* tt2, c
             bulk_load(sm.b1(b ^ 1), v1 + ((size_t)(c + 1) << kTileLog), kTileBytes1, &sm.bar[b ^ 1]);
         }
         const bool got = mbar_wait(&sm.bar[b], ph);
-        if (__syncthreads_or(!got)) {
+        if (gsync_or<NT>(!got)) {
             // Give the copies of tiles c and c + 1 one more bounded wait before leaving.
-            if (threadIdx.x == 0) {
+            if (gtid<NT>() == 0) {
                 mbar_wait(&sm.bar[b], ph);
                 if (c + 1 < tiles) mbar_wait(&sm.bar[b ^ 1], ((par >> (b ^ 1)) ^ (uint32_t)((c + 1) >> 1)) & 1);
             }
@@ -342,18 +346,18 @@ __device__ __noinline__ bool tile_phase(F2* v2, F1* v1, int n, const F2K* tt2, c
         // Generic accesses of this buffer before the async proxy reads (store) or rewrites
         // (the load of tile c + 2) it.
         fence_async_shared();
-        __syncthreads();
-        if (store && threadIdx.x == 0) {
+        gsync<NT>();
+        if (store && gtid<NT>() == 0) {
             bulk_store(v2 + ((size_t)c << kTileLog), s2, kTileBytes2);
             bulk_store(v1 + ((size_t)c << kTileLog), s1, kTileBytes1);
             bulk_commit();
         }
     }
-    if (threadIdx.x == 0) {
+    if (gtid<NT>() == 0) {
         bulk_wait_all();
         fence_async_global();
     }
-    __syncthreads();
+    gsync<NT>();
     return ok;
 }
 
@@ -364,7 +368,7 @@ template <int NT, class COEF>
 __device__ __forceinline__ uint64_t chunked_sum(const COEF& coef, int count, uint32_t* out, uint64_t cin, uint64_t* sc) {
 #pragma unroll 1
     for (int base = 0; base < count; base += kChunkE * NT) {
-        const int q0 = base + threadIdx.x * kChunkE;
+        const int q0 = base + gtid<NT>() * kChunkE;
         uint32_t L[kChunkE];
         Acc96 acc;
 #pragma unroll
@@ -377,7 +381,7 @@ __device__ __forceinline__ uint64_t chunked_sum(const COEF& coef, int count, uin
 #pragma unroll
         for (int e = 0; e < kChunkE; ++e) out[q0 + e] = L[e];
     }
-    __syncthreads();
+    gsync<NT>();
     return cin;
 }
 
@@ -398,7 +402,7 @@ __device__ __noinline__ void g_carry_low_and_pack(F2* v2, F1* v1, int n, uint64_
     uint64_t cin = 0;
 #pragma unroll 1
     for (int base = 0; base < n; base += kChunkE * NT) {
-        const int q0 = base + threadIdx.x * kChunkE;
+        const int q0 = base + gtid<NT>() * kChunkE;
         uint32_t L[kChunkE];
         Acc96 acc;
 #pragma unroll
@@ -419,7 +423,7 @@ __device__ __noinline__ void g_carry_low_and_pack(F2* v2, F1* v1, int n, uint64_
             v1[j] = z1;
         }
     }
-    __syncthreads();
+    gsync<NT>();
 }
 
 template <int NT>
@@ -447,8 +451,8 @@ __device__ __noinline__ bool g_wrap_combine(const F2* v2, const F1* v1, int n, c
 template <int NT>
 __device__ __noinline__ void half_pointwise_rt(F2* v2, F1* v1, int H, const F2* __restrict__ ab2, const F1* __restrict__ ab1) {
 #pragma unroll 1
-    for (int tau = threadIdx.x; tau < H / 2 + 1; tau += NT) half_pointwise_pair(v2, v1, H, ab2, ab1, tau);
-    __syncthreads();
+    for (int tau = gtid<NT>(); tau < H / 2 + 1; tau += NT) half_pointwise_pair(v2, v1, H, ab2, ab1, tau);
+    gsync<NT>();
 }
 
 // ---- the REDC without the wraparound path on global vectors ----
@@ -458,7 +462,7 @@ __device__ __noinline__ void g_carry_low_to(const F2* v2, const F1* v1, int n, u
     uint64_t cin = 0;
 #pragma unroll 1
     for (int base = 0; base < k; base += kChunkE * NT) {
-        const int q0 = base + threadIdx.x * kChunkE;
+        const int q0 = base + gtid<NT>() * kChunkE;
         uint32_t L[kChunkE];
         Acc96 acc;
 #pragma unroll
@@ -475,7 +479,7 @@ __device__ __noinline__ void g_carry_low_to(const F2* v2, const F1* v1, int n, u
         for (int e = 0; e < kChunkE; ++e)
             if (q0 + e < k) out[q0 + e] = L[e];
     }
-    __syncthreads();
+    gsync<NT>();
 }
 
 // x = (T + m N) / R, as carry_shift_add, in chunks over the 2n coefficients of m N.
@@ -486,7 +490,7 @@ __device__ __noinline__ bool g_carry_shift_add(const F2* v2, const F1* v1, int n
     uint64_t cin = 0;
 #pragma unroll 1
     for (int base = 0; base < 2 * n; base += kChunkE * NT) {
-        const int q0 = base + threadIdx.x * kChunkE;
+        const int q0 = base + gtid<NT>() * kChunkE;
         uint32_t L[kChunkE];
         Acc96 acc;
 #pragma unroll
@@ -509,7 +513,7 @@ __device__ __noinline__ bool g_carry_shift_add(const F2* v2, const F1* v1, int n
             else if (q >= 2 * k) stray |= L[e] != 0;
         }
     }
-    return !__syncthreads_or(stray) && cin == 0;
+    return !gsync_or<NT>(stray) && cin == 0;
 }
 
 // ---- the wraparound steps on global vectors ----
@@ -552,8 +556,8 @@ __device__ __forceinline__ int g_redc_plain(F2* w2, F1* w1, int m, const uint32_
     const F2K* tt2 = tab2 + glt_tile_off(m);
     const F1* tt1 = tab1 + glt_tile_off(m);
     int nz = 0;
-    for (int q = threadIdx.x; q < k; q += NT) nz |= tl[q] != 0;
-    const uint32_t flag = __syncthreads_or(nz) ? 1u : 0u;
+    for (int q = gtid<NT>(); q < k; q += NT) nz |= tl[q] != 0;
+    const uint32_t flag = gsync_or<NT>(nz) ? 1u : 0u;
     g_fwd<NT>(m, true, tl, w2, w1, tab2, tab1, k);
     if (!tile_phase<NT>(w2, w1, n, tt2, tt1, SpecMulRT{cc2, cc1, n / 8}, kTileFull, sm, par)) return kStepTimeout;
     par = tile_par_next(par, n);
@@ -601,8 +605,8 @@ __device__ __forceinline__ bool gstep_slot(const GArgs& g, uint32_t slot, uint32
         if (st == kStepTimeout) break;
         carry_ok &= st == kStepOk;
     }
-    __syncthreads();   // every thread has read pos before it is written
-    if (threadIdx.x == 0) {
+    gsync<NT>();   // every thread has read pos before it is written
+    if (gtid<NT>() == 0) {
         a.pos[slot] = pos;
         if (st == kStepTimeout) a.err[slot] = kErrTimeout;
         else if (!carry_ok) a.err[slot] = 1;
@@ -617,7 +621,7 @@ __global__ void __launch_bounds__(NT, 2) gstep_kernel(GArgs g, uint32_t first, u
     __shared__ uint64_t sc[CarryScratch<NT>::words];
     __shared__ uint64_t bars[2];
     const TileSmem sm{smem_raw, bars};
-    tile_init(sm);
+    tile_init<NT>(sm);
     uint32_t par = 0;
     gstep_slot<NT>(g, first + blockIdx.x, bits, sm, sc, par);
 }
@@ -629,7 +633,7 @@ __global__ void __launch_bounds__(NT, 2) gmul_kernel(GArgs g, uint32_t out, uint
     __shared__ uint64_t sc[CarryScratch<NT>::words];
     __shared__ uint64_t bars[2];
     const TileSmem sm{smem_raw, bars};
-    tile_init(sm);
+    tile_init<NT>(sm);
     const SlotArgs& a = g.a;
     const int m = g.m, n = 1 << m;
     F2* w2 = g.w2 + (size_t)out * n;
@@ -656,7 +660,7 @@ __global__ void __launch_bounds__(NT, 2) gmul_kernel(GArgs g, uint32_t out, uint
             if (st == kStepOk && !fits) st = kStepCarry;
         }
     }
-    if (threadIdx.x == 0 && st != kStepOk) a.err[out] = st == kStepTimeout ? kErrTimeout : 1;
+    if (gtid<NT>() == 0 && st != kStepOk) a.err[out] = st == kStepTimeout ? kErrTimeout : 1;
 }
 
 // Per-slot constants in global mode (as setup_kernel): F(N') through the global passes and the
@@ -667,7 +671,7 @@ __global__ void __launch_bounds__(NT, 2) gsetup_kernel(GArgs g, const uint32_t* 
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ uint64_t bars[2];
     const TileSmem sm{smem_raw, bars};
-    tile_init(sm);
+    tile_init<NT>(sm);
     const SlotArgs& a = g.a;
     const int m = g.m, n = 1 << m, h = n / 2;
     const uint32_t slot = slots ? slots[blockIdx.x] : first + blockIdx.x;
@@ -689,7 +693,7 @@ __global__ void __launch_bounds__(NT, 2) gsetup_kernel(GArgs g, const uint32_t* 
             g_fwd<NT>(m, true, nl + row * k, w2, w1, a.tab2, a.tab1, k);
             ok = tile_phase<NT>(w2, w1, n, tt2, tt1, SpecStoreRT{o2 + n, o1 + n, n / 8}, kTileDifOp, sm, par);
         }
-        if (threadIdx.x == 0 && !ok) a.err[slot] = kErrTimeout;
+        if (gtid<NT>() == 0 && !ok) a.err[slot] = kErrTimeout;
         return;
     }
     if (tile_phase<NT>(w2, w1, n, tt2, tt1, SpecStoreRT{o2, o1, n / 8}, kTileDifOp, sm, par)) {
@@ -704,7 +708,7 @@ __global__ void __launch_bounds__(NT, 2) gsetup_kernel(GArgs g, const uint32_t* 
             ok = true;
         }
     }
-    if (threadIdx.x == 0 && !ok) a.err[slot] = kErrTimeout;
+    if (gtid<NT>() == 0 && !ok) a.err[slot] = kErrTimeout;
 }
 
 // The Transform trait's forward or inverse of vector first + blockIdx.x in global mode, in place
@@ -716,7 +720,7 @@ __global__ void __launch_bounds__(NT, 2) gtransform_kernel(F2* v2, F1* v1, const
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ uint64_t bars[2];
     const TileSmem sm{smem_raw, bars};
-    tile_init(sm);
+    tile_init<NT>(sm);
     const int n = 1 << m, P = gl_passes(m);
     F2* w2 = v2 + (size_t)(first + blockIdx.x) * n;
     F1* w1 = v1 + (size_t)(first + blockIdx.x) * n;
@@ -741,8 +745,8 @@ __global__ void __launch_bounds__(NT, 2) gtransform_kernel(F2* v2, F1* v1, const
         if (ok) g_inv<NT, false>(m, true, w2, w1, tab2, tab1);
     }
     if (ok)
-        for (int e = threadIdx.x; e < n; e += NT) w2[e] = lccanon(w2[e]);
-    if (threadIdx.x == 0 && !ok) *err = kErrTimeout;
+        for (int e = gtid<NT>(); e < n; e += NT) w2[e] = lccanon(w2[e]);
+    if (gtid<NT>() == 0 && !ok) *err = kErrTimeout;
 }
 
 }  // namespace mm

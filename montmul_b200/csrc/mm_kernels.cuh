@@ -99,8 +99,8 @@ template <int MH, int NT>
 __device__ __noinline__ void half_pointwise(F2* s2, F1* s1, const F2* __restrict__ ab2, const F1* __restrict__ ab1) {
     constexpr int H = 1 << MH;
 #pragma unroll 1
-    for (int tau = threadIdx.x; tau < H / 2 + 1; tau += NT) half_pointwise_pair(s2, s1, H, ab2, ab1, tau);
-    __syncthreads();
+    for (int tau = gtid<NT>(); tau < H / 2 + 1; tau += NT) half_pointwise_pair(s2, s1, H, ab2, ab1, tau);
+    gsync<NT>();
 }
 
 // half_forward's packing (cpu.rs:286-295): z_j = v_2j + i v_2j+1 for j < h, at swz(j). Ends
@@ -175,11 +175,11 @@ __global__ void __launch_bounds__(NT) transform_kernel(F2* v2, F1* v1, const F2K
     F1* s1 = reinterpret_cast<F1*>(smem_raw + 16 * N);
     F2* g2 = v2 + (size_t)(first + blockIdx.x) * N;
     F1* g1 = v1 + (size_t)(first + blockIdx.x) * N;
-    for (int e = threadIdx.x; e < N; e += NT) {
+    for (int e = gtid<NT>(); e < N; e += NT) {
         s2[e] = g2[e];
         s1[e] = g1[e];
     }
-    __syncthreads();
+    gsync<NT>();
     if (!inverse) {
         dif_first_complex<M, NT>(s2, s1, tab2, tab1);
         if constexpr (P >= 2) smem_pass<M, (P >= 2 ? 1 : 0), true, NT, true>(s2, s1, tab2, tab1);
@@ -193,7 +193,7 @@ __global__ void __launch_bounds__(NT) transform_kernel(F2* v2, F1* v1, const F2K
         if constexpr (P >= 2) smem_pass<M, (P >= 2 ? 1 : 0), false, NT, true>(s2, s1, tab2, tab1);
         dit_last_complex<M, NT>(s2, s1, tab2, tab1);
     }
-    for (int e = threadIdx.x; e < N; e += NT) {
+    for (int e = gtid<NT>(); e < N; e += NT) {
         g2[e] = lccanon(s2[e]);
         g1[e] = s1[e];
     }
@@ -228,8 +228,8 @@ __device__ __noinline__ bool redc_plain(F2* s2, F1* s1, const uint32_t* tl, uint
                                         const F2K* tab2, const F1* tab1, uint64_t* sc, int k) {
     constexpr int N = 1 << M;
     int nz = 0;
-    for (int q = threadIdx.x; q < k; q += NT) nz |= tl[q] != 0;
-    const uint32_t flag = __syncthreads_or(nz) ? 1u : 0u;
+    for (int q = gtid<NT>(); q < k; q += NT) nz |= tl[q] != 0;
+    const uint32_t flag = gsync_or<NT>(nz) ? 1u : 0u;
     fwd_limbs<M, NT>(tl, k, s2, s1, tab2, tab1);
     fused_mid<M, NT, true>(tl, k, s2, s1, tab2, tab1, SpecMulOp<M>{cc2, cc1});
     inv_to_natural<M, NT, true>(s2, s1, tab2, tab1);
@@ -270,8 +270,8 @@ __device__ __forceinline__ void step_slot(const SlotArgs& a, uint32_t slot, uint
         if (a.plain) ok &= redc_plain<M, NT>(s2, s1, tl, x, cc2, cc1, a.tab2, a.tab1, sc, k);
         else ok &= redc_wrap<M, NT>(s2, s1, tl, x, cc2, cc1, a.tab2, a.tab1, sc);
     }
-    __syncthreads();   // every thread has read pos before it is written
-    if (threadIdx.x == 0) {
+    gsync<NT>();   // every thread has read pos before it is written
+    if (gtid<NT>() == 0) {
         a.pos[slot] = pos;
         if (!ok) a.err[slot] = 1;
     }
@@ -299,7 +299,7 @@ __global__ void __launch_bounds__(NT) mul_kernel(SlotArgs a, uint32_t out, uint3
     const uint32_t* xa = a.x + (size_t)ia * k;
     fwd_limbs<M, NT>(xb, k, s2, s1, a.tab2, a.tab1);
     fused_mid<M, NT, false>(xb, k, s2, s1, a.tab2, a.tab1, SpecStoreOp<M>{spec2, spec1});
-    __syncthreads();
+    gsync<NT>();
     fwd_limbs<M, NT>(xa, k, s2, s1, a.tab2, a.tab1);
     fused_mid<M, NT, false>(xa, k, s2, s1, a.tab2, a.tab1, SpecMulOp<M>{spec2, spec1});
     inv_to_natural<M, NT, false>(s2, s1, a.tab2, a.tab1);
@@ -311,7 +311,7 @@ __global__ void __launch_bounds__(NT) mul_kernel(SlotArgs a, uint32_t out, uint3
                                 sc, k);
     else
         ok &= redc_wrap<M, NT>(s2, s1, tl, xo, a.c2 + (size_t)out * 2 * N, a.c1 + (size_t)out * 2 * N, a.tab2, a.tab1, sc);
-    if (threadIdx.x == 0 && !ok) a.err[out] = 1;
+    if (gtid<NT>() == 0 && !ok) a.err[out] = 1;
 }
 
 // Per-slot constants of slot first + blockIdx.x (or slots[blockIdx.x]) from its N and N' limbs
@@ -337,7 +337,7 @@ __global__ void __launch_bounds__(NT) setup_kernel(const uint32_t* nl, const uin
     F1* o1 = c1 + (size_t)slot * 2 * N;
     fwd_limbs<M, NT>(np, (int)k, s2, s1, tab2, tab1);
     fused_mid<M, NT, false>(np, (int)k, s2, s1, tab2, tab1, SpecStoreOp<M>{o2, o1});
-    __syncthreads();
+    gsync<NT>();
     if (plain) {
         // F(N) in the second half (cpu.rs:518-521), in fused-pass order.
         fwd_limbs<M, NT>(nn, (int)k, s2, s1, tab2, tab1);

@@ -1,12 +1,15 @@
 // The mixed-length persistent launch: slots of several batches (each batch one transform length)
-// run in one launch whose blocks take work items from a device counter. One item = every step
-// (up to `bits`) of one slot, so a block stays on a slot until it is done with it and then
+// run in one launch whose blocks take work items from device counters. One item = every step
+// (up to `bits`) of one slot, so a worker stays on a slot until it is done with it and then
 // takes the next item; the host orders the items longest first, which bounds the tail of the
 // launch by the cost of one of the shortest items.
 //
-// Every block has 256 threads and 96 KiB of dynamic shared memory (two blocks per SM): lengths
-// with n <= 4096 run with the whole vector in shared memory, longer ones in global mode. There
-// is no counterpart in the reference, whose launches each cover one batch of one length
+// One block per SM: 512 threads and 192 KiB of dynamic shared memory. The block first takes the
+// wide items (L = 16384 in shared mode: all 512 threads and all of the shared memory on one
+// slot), then splits into two groups of 256 threads, each with its own 96 KiB and hardware
+// barrier, which take the other items independently: lengths with n <= 4096 with the whole
+// vector in shared memory, longer ones (and batches tuned to it) in global mode. There is no
+// counterpart in the reference, whose launches each cover one batch of one length
 // (montmul/src/gpu/mod.rs:119-158).
 #include "mm_global.cuh"
 
@@ -15,47 +18,74 @@ namespace mm {
 // One slot of a shared-mode batch; one function per length keeps each length's register
 // allocation separate from the dispatch.
 template <int M>
-__device__ __noinline__ void mixed_shared(const SlotArgs& a, uint32_t slot, uint32_t bits, unsigned char* smem_raw,
+__device__ __noinline__ void mixed_shared(const SlotArgs& a, uint32_t slot, uint32_t bits, unsigned char* smem,
                                           uint64_t* sc) {
-    step_slot<M, kMixedThreads>(a, slot, bits, smem_raw, sc);
+    step_slot<M, kMixedThreads>(a, slot, bits, smem, sc);
 }
 
-__global__ void __launch_bounds__(kMixedThreads, 2)
-    mixed_step_kernel(const MixedDesc* __restrict__ descs, const uint4* __restrict__ items,
-                      const uint32_t* __restrict__ count_ptr, uint32_t* counter, uint32_t bits) {
+__device__ __noinline__ void mixed_wide(const SlotArgs& a, uint32_t slot, uint32_t bits, unsigned char* smem,
+                                        uint64_t* sc) {
+    step_slot<kWideLogN, kWideThreads>(a, slot, bits, smem, sc);
+}
+
+constexpr int kGroupScratch = CarryScratch<kMixedThreads>::words;
+constexpr int kScratchWords = cmax(kMixedGroups * kGroupScratch, CarryScratch<kWideThreads>::words);
+
+__device__ __forceinline__ uint32_t item_steps(const uint4& it, const MixedDesc& d, uint32_t bits) {
+    return it.z ? it.z : (d.bits ? d.bits : bits);
+}
+
+__global__ void __launch_bounds__(kMixedBlockThreads, 1)
+    mixed_step_kernel(const MixedDesc* __restrict__ descs, MixedLists l, uint32_t bits) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ uint64_t sc[CarryScratch<kMixedThreads>::words];
-    __shared__ uint64_t bars[2];
-    __shared__ uint32_t next;
-    const TileSmem sm{smem_raw, bars};
-    tile_init(sm);
-    uint32_t par = 0;
-    const uint32_t count = *count_ptr;
-    for (;;) {
-        if (threadIdx.x == 0) next = atomicAdd(counter, 1u);
+    __shared__ uint64_t sc[kScratchWords];
+    __shared__ uint64_t bars[kMixedGroups][2];
+    __shared__ uint32_t next[kMixedGroups];
+    // Wide items: the whole block on one slot.
+    const uint32_t wide_count = *l.wide_count;
+    while (wide_count) {
+        if (threadIdx.x == 0) next[0] = atomicAdd(&l.counter[1], 1u);
         __syncthreads();
-        const uint32_t i = next;
+        const uint32_t i = next[0];
         __syncthreads();   // every thread has read `next` before thread 0 takes the next item
-        if (i >= count) break;
-        const uint4 it = items[i];
+        if (i >= wide_count) break;
+        const uint4 it = l.wide[i];
         const MixedDesc& d = descs[it.x];
-        const uint32_t steps = it.z ? it.z : (d.bits ? d.bits : bits);
+        mixed_wide(d.g.a, it.y, item_steps(it, d, bits), smem_raw, sc);
+    }
+    // The other items: two groups, each on its own slots with its own half of the memory.
+    const int grp = threadIdx.x / kMixedThreads;
+    unsigned char* gsm = smem_raw + grp * kMixedGroupSmem;
+    uint64_t* gsc = sc + grp * kGroupScratch;
+    const TileSmem sm{gsm, bars[grp]};
+    tile_init<kMixedThreads>(sm);
+    uint32_t par = 0;
+    const uint32_t count = *l.count;
+    for (;;) {
+        if (gtid<kMixedThreads>() == 0) next[grp] = atomicAdd(&l.counter[0], 1u);
+        gsync<kMixedThreads>();
+        const uint32_t i = next[grp];
+        gsync<kMixedThreads>();   // the group has read `next` before its thread 0 takes the next item
+        if (i >= count) break;
+        const uint4 it = l.items[i];
+        const MixedDesc& d = descs[it.x];
+        const uint32_t steps = item_steps(it, d, bits);
         if (d.global) {
-            if (!gstep_slot<kMixedThreads>(d.g, it.y, steps, sm, sc, par)) break;
+            if (!gstep_slot<kMixedThreads>(d.g, it.y, steps, sm, gsc, par)) break;
             continue;
         }
         switch (d.g.m) {
-            case 2: mixed_shared<2>(d.g.a, it.y, steps, smem_raw, sc); break;
-            case 3: mixed_shared<3>(d.g.a, it.y, steps, smem_raw, sc); break;
-            case 4: mixed_shared<4>(d.g.a, it.y, steps, smem_raw, sc); break;
-            case 5: mixed_shared<5>(d.g.a, it.y, steps, smem_raw, sc); break;
-            case 6: mixed_shared<6>(d.g.a, it.y, steps, smem_raw, sc); break;
-            case 7: mixed_shared<7>(d.g.a, it.y, steps, smem_raw, sc); break;
-            case 8: mixed_shared<8>(d.g.a, it.y, steps, smem_raw, sc); break;
-            case 9: mixed_shared<9>(d.g.a, it.y, steps, smem_raw, sc); break;
-            case 10: mixed_shared<10>(d.g.a, it.y, steps, smem_raw, sc); break;
-            case 11: mixed_shared<11>(d.g.a, it.y, steps, smem_raw, sc); break;
-            case 12: mixed_shared<12>(d.g.a, it.y, steps, smem_raw, sc); break;
+            case 2: mixed_shared<2>(d.g.a, it.y, steps, gsm, gsc); break;
+            case 3: mixed_shared<3>(d.g.a, it.y, steps, gsm, gsc); break;
+            case 4: mixed_shared<4>(d.g.a, it.y, steps, gsm, gsc); break;
+            case 5: mixed_shared<5>(d.g.a, it.y, steps, gsm, gsc); break;
+            case 6: mixed_shared<6>(d.g.a, it.y, steps, gsm, gsc); break;
+            case 7: mixed_shared<7>(d.g.a, it.y, steps, gsm, gsc); break;
+            case 8: mixed_shared<8>(d.g.a, it.y, steps, gsm, gsc); break;
+            case 9: mixed_shared<9>(d.g.a, it.y, steps, gsm, gsc); break;
+            case 10: mixed_shared<10>(d.g.a, it.y, steps, gsm, gsc); break;
+            case 11: mixed_shared<11>(d.g.a, it.y, steps, gsm, gsc); break;
+            case 12: mixed_shared<12>(d.g.a, it.y, steps, gsm, gsc); break;
             default: break;   // the host never builds such a descriptor
         }
     }

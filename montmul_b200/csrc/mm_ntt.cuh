@@ -17,6 +17,27 @@
 
 namespace mm {
 
+// ---- thread groups ----
+// One slot is worked on by a group of NT threads (NT a power of two, a multiple of 32). A block
+// is one group (the uniform launches) or several (the mixed launch runs two groups of 256 per
+// block). Group g synchronizes on hardware barrier 1 + g with its NT threads only, so the groups
+// of a block run independently.
+template <int NT> __device__ __forceinline__ int gtid() { return (int)(threadIdx.x & (NT - 1)); }
+template <int NT> __device__ __forceinline__ int gbar() { return 1 + (int)(threadIdx.x / NT); }
+template <int NT> __device__ __forceinline__ void gsync() {
+    asm volatile("bar.sync %0, %1;" ::"r"(gbar<NT>()), "n"(NT) : "memory");
+}
+// Barrier of the group that returns whether `pred` is non-zero on any of its threads.
+template <int NT> __device__ __forceinline__ int gsync_or(int pred) {
+    int r;
+    asm volatile(
+        "{ .reg .pred p, q; setp.ne.s32 p, %1, 0; bar.red.or.pred q, %2, %3, p; selp.s32 %0, 1, 0, q; }"
+        : "=r"(r)
+        : "r"(pred), "r"(gbar<NT>()), "n"(NT)
+        : "memory");
+    return r;
+}
+
 __device__ __forceinline__ int swz(int e) {
     return (e & ~15) | ((((e >> 3) ^ (e >> 6)) & 1) << 3) | ((e ^ (e >> 3)) & 7);
 }
@@ -153,7 +174,7 @@ __device__ __noinline__ void pass_rt(F2* s2, F1* s1, const F2K* __restrict__ t2,
 #pragma unroll
     for (int k = 0; k < R; ++k) ko[k] = swz(k * q);
 #pragma unroll 1
-    for (int g = threadIdx.x; g < G; g += NT) {
+    for (int g = gtid<NT>(); g < G; g += NT) {
         const int j = g & (q - 1);
         // b + k q has disjoint bits, and swz is linear over XOR: swz(b + k q) = swz(b) ^ swz(k q).
         const int sb = swz(((g >> LQ) << (LQ + ilog2c(R))) + j);
@@ -197,7 +218,7 @@ __device__ __noinline__ void pass_rt(F2* s2, F1* s1, const F2K* __restrict__ t2,
             for (int k = 0; k < R; ++k) s1[sb ^ ko[k]] = x[k];
         }
     }
-    __syncthreads();
+    gsync<NT>();
 }
 
 // Pass I (DIF order) of the length-2^M transform; its table follows mm_common.h's layout.
@@ -226,7 +247,7 @@ __device__ __noinline__ void dif_first_from_limbs(const uint32_t* __restrict__ l
     static_assert(Q > 1, "single-pass transforms use the fused pass");
     constexpr int toff = tab_fwd_off(M, 0, true), coff = tab_in_const_off(M, true);
 #pragma unroll 1
-    for (int j = threadIdx.x; j < Q; j += NT) {
+    for (int j = gtid<NT>(); j < Q; j += NT) {
         uint32_t v[R];
 #pragma unroll
         for (int k = 0; k < R; ++k) v[k] = (j + k * Q < cnt) ? lim[j + k * Q] : 0u;
@@ -247,7 +268,7 @@ __device__ __noinline__ void dif_first_from_limbs(const uint32_t* __restrict__ l
             for (int k = 0; k < R; ++k) s1[swz(j + k * Q)] = cmul(x[k], tab1[toff + k * Q + j]);
         }
     }
-    __syncthreads();
+    gsync<NT>();
 }
 
 // ---- the weighted last DIT pass: unweights by zeta^-(j + k q) / n into natural order ----
@@ -258,7 +279,7 @@ __device__ __noinline__ void dit_last_weighted(F2* s2, F1* s1, const F2K* tab2, 
     static_assert(Q > 1, "single-pass transforms use the fused pass");
     constexpr int toff = tab_inv_off(M, 0, true), coff = tab_out_const_off(M, true);
 #pragma unroll 1
-    for (int j = threadIdx.x; j < Q; j += NT) {
+    for (int j = gtid<NT>(); j < Q; j += NT) {
         {
             F2 x[R];
 #pragma unroll
@@ -282,7 +303,7 @@ __device__ __noinline__ void dit_last_weighted(F2* s2, F1* s1, const F2K* tab2, 
             }
         }
     }
-    __syncthreads();
+    gsync<NT>();
 }
 
 // ---- the Transform trait's weighted passes on complex elements (cpu.rs:86-103) ----
@@ -294,7 +315,7 @@ __device__ __noinline__ void dif_first_complex(F2* s2, F1* s1, const F2K* tab2, 
     constexpr int R = sched_radix(M, 0), Q = sched_q(M, 0);
     constexpr int toff = tab_fwd_off(M, 0, true), coff = tab_in_const_off(M, true);
 #pragma unroll 1
-    for (int j = threadIdx.x; j < Q; j += NT) {
+    for (int j = gtid<NT>(); j < Q; j += NT) {
         {
             F2 x[R];
 #pragma unroll
@@ -313,7 +334,7 @@ __device__ __noinline__ void dif_first_complex(F2* s2, F1* s1, const F2K* tab2, 
             for (int k = 0; k < R; ++k) s1[swz(j + k * Q)] = Q > 1 ? cmul(x[k], tab1[toff + k * Q + j]) : x[k];
         }
     }
-    __syncthreads();
+    gsync<NT>();
 }
 
 // Inverse: the pass twiddles (with zeta^-j) before the butterfly, zeta^-(q k) / n after it.
@@ -322,7 +343,7 @@ __device__ __noinline__ void dit_last_complex(F2* s2, F1* s1, const F2K* tab2, c
     constexpr int R = sched_radix(M, 0), Q = sched_q(M, 0);
     constexpr int toff = tab_inv_off(M, 0, true), coff = tab_out_const_off(M, true);
 #pragma unroll 1
-    for (int j = threadIdx.x; j < Q; j += NT) {
+    for (int j = gtid<NT>(); j < Q; j += NT) {
         {
             F2 x[R];
 #pragma unroll
@@ -341,7 +362,7 @@ __device__ __noinline__ void dit_last_complex(F2* s2, F1* s1, const F2K* tab2, c
             for (int k = 0; k < R; ++k) s1[swz(j + k * Q)] = cmul(x[k], tab1[coff + k]);
         }
     }
-    __syncthreads();
+    gsync<NT>();
 }
 
 // ---- the fused middle: last DIF pass (span 1), a pointwise operation, first DIT pass ----
@@ -356,7 +377,7 @@ __device__ __noinline__ void fused_mid(const uint32_t* __restrict__ lim, int cnt
     constexpr bool single = (P == 1);
     constexpr int cin = tab_in_const_off(M, true), cout = tab_out_const_off(M, true);
 #pragma unroll 1
-    for (int g = threadIdx.x; g < G; g += NT) {
+    for (int g = gtid<NT>(); g < G; g += NT) {
         {
             F2 x[R];
             if (single) {
@@ -406,7 +427,7 @@ __device__ __noinline__ void fused_mid(const uint32_t* __restrict__ lim, int cnt
             }
         }
     }
-    __syncthreads();
+    gsync<NT>();
 }
 
 // ---- whole transforms ----

@@ -188,19 +188,14 @@ class Server:
 
     # ---- ticks ----
     def mixed_step_ns(self, length: int) -> float:
-        """Cost of one slot-step of a length in the mixed launch, from the tuned table: shared
-        mode up to L = 8192, global mode above (the mixed launch's blocks hold 96 KiB)."""
+        """Cost of one slot-step of a length in the mixed launch (GPU time per slot-step with
+        the whole GPU on that length), from the tuned table: the measured cost inside the mixed
+        launch, else the uniform launch's."""
         row = self.table.get(str(length))
         if not row:
             n = length // 2
             return float(n * max(1, n.bit_length() - 1))
-        if "mixed_ns" in row:
-            return row["mixed_ns"]
-        if length > 8192:
-            g = [c["step_ns"] for c in row.get("candidates", []) if c["global"]]
-            if g:
-                return min(g)
-        return row["step_ns"]
+        return row.get("mixed_ns", row["step_ns"])
 
     def _plan(self):
         from .backend import Plan
@@ -210,36 +205,45 @@ class Server:
             segs = [s for L in sorted(self.lanes) for s in self.lanes[L]]
             self.plan = Plan([s.batch for s in segs], self.quantum)
             self.plan_segs = segs
-            # Every length gets the steps that take as long as `quantum` steps of the costliest
-            # one, so no block idles while the longest items of a tick finish.
-            costs = [self.mixed_step_ns(s.batch.params.len) for s in segs]
-            top = max(costs)
-            self.seg_ns = costs
-            self.seg_steps = [max(1, int(round(self.quantum * top / c))) for c in costs]
+            # An item's time per step on its worker is the GPU-wide cost per slot-step times the
+            # workers sharing the GPU: a wide item (L = 16384) holds a whole block, the others
+            # one of its two workers. Every length gets the steps that take as long as
+            # `quantum` steps of the slowest, so no worker idles while the longest items of a
+            # tick finish.
             self.blocks = self.plan.blocks()
+            wide_blocks = self.plan.wide_blocks()
+            wide = [self.plan.batch_wide(i) for i in range(len(segs))]
+            self.seg_units = [max(1, self.blocks // wide_blocks) if w else 1 for w in wide]
+            self.seg_ns = [self.mixed_step_ns(s.batch.params.len) * (wide_blocks if w else self.blocks)
+                           for s, w in zip(segs, wide)]
+            top = max(self.seg_ns)
+            self.seg_steps = [max(1, int(round(self.quantum * top / c))) for c in self.seg_ns]
             self.plan_dirty = False
         return self.plan
 
     def work_list(self):
-        """This tick's items (plan batch, slot, steps), longest first. With up to as many busy
-        slots as resident blocks each takes a full budget (the same time for every length). With
-        more, A = q W + r busy slots (0 < r <= W blocks) split into (W - r) q items of 1/q of a
-        budget and r (q + 1) items of 1/(q + 1), so every block ends the tick at once (exactly
-        for q = 1); the slots nearest completion get the larger shares."""
+        """This tick's items (plan batch, slot, steps), longest first. Items are counted in
+        worker units (a wide item holds the two workers of a block). With up to as many units as
+        workers each item takes a full budget (the same time for every length). With more,
+        A = q W + r units (0 < r <= W workers) split into (W - r) q units of 1/q of a budget and
+        r (q + 1) units of 1/(q + 1), so every worker ends the tick at once (exactly for q = 1
+        and no wide items); the slots nearest completion get the larger shares."""
         items = []
         for si, seg in enumerate(self.plan_segs):
             for s in seg.active:
                 rem = seg.batch.remaining(s)
-                items.append([si, s, self.seg_steps[si], rem, self.seg_ns[si]])
-        a, w = len(items), max(1, self.blocks)
+                items.append([si, s, self.seg_steps[si], rem, self.seg_ns[si], self.seg_units[si]])
+        a, w = sum(it[5] for it in items), max(1, self.blocks)
         if a > w:
             q, r = divmod(a, w)
             if r == 0:
                 q, r = q - 1, w
             big = (w - r) * q
             items.sort(key=lambda it: it[3] * it[4])
-            for i, it in enumerate(items):
-                it[2] = max(1, it[2] // (q if i < big else q + 1))
+            units = 0
+            for it in items:
+                it[2] = max(1, it[2] // (q if units < big else q + 1))
+                units += it[5]
         for it in items:
             it[2] = max(1, min(it[2], it[3]))
         items.sort(key=lambda it: -it[2] * it[4])

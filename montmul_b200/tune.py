@@ -110,8 +110,9 @@ def measure(dev, length: int, global_mode: bool, launch_steps: int, slots: int, 
 
 
 def measure_mixed(dev, length: int, slots: int, steps: int, seed: int = 2026):
-    """Seconds per slot-step of one length inside the mixed-length persistent launch (256-thread
-    blocks, two per SM; global mode above L = 8192), at full occupancy: the cost that orders a
+    """Seconds per slot-step of one length inside the mixed-length persistent launch (one
+    512-thread block per SM: L = 16384 as wide items on whole blocks, shorter lengths on its two
+    256-thread workers, longer ones in global mode), at full occupancy: the cost that orders a
     mixed launch's items and sizes a serving tick's budgets."""
     from .backend import Plan
     from .batch import ModBatch
@@ -192,13 +193,18 @@ def apply(batch, table=None) -> bool:
     return True
 
 
-def tune(dev, lengths, force: bool = False, log=print):
+def tune(dev, lengths, force: bool = False, log=print, mixed_only: bool = False):
+    """Measures the schedule of every length not in the table (all with `force`), and each
+    length's cost inside the mixed launch where the table lacks it (all with `mixed_only`, which
+    keeps the schedules)."""
     table = load_table()
     name = dev.device_name()
     per = table.setdefault(name, {})
     for length in lengths:
         row = per.get(str(length))
-        if row and not force:
+        if row and mixed_only:
+            row.pop("mixed_ns", None)
+        if row and (mixed_only or not force):
             if "mixed_ns" not in row and length <= MAX_MIXED_L:
                 steps = max(8, min(int(row.get("steps", 64)), 1000))
                 row["mixed_ns"] = measure_mixed(dev, length, int(row.get("slots", 8 * dev.sm_count())), steps) * 1e9
@@ -217,11 +223,13 @@ def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--lengths", type=int, nargs="*", default=[1 << e for e in range(8, 18)])
     ap.add_argument("--force", action="store_true", help="re-measure lengths already in the table")
+    ap.add_argument("--mixed-only", action="store_true",
+                    help="keep the schedules and re-measure only each length's cost inside the mixed launch")
     ap.add_argument("--device", type=int, default=0)
     a = ap.parse_args(argv)
     from .backend import B200
     dev = B200(device=a.device)
-    per = tune(dev, a.lengths, a.force)
+    per = tune(dev, a.lengths, a.force, mixed_only=a.mixed_only)
     print(json.dumps({str(k): {kk: v for kk, v in per[str(k)].items() if kk != "candidates"} for k in a.lengths}))
     return 0
 

@@ -197,7 +197,8 @@ def test_plan_run_items_lists(dev):
     spec = _batches(dev, [4000, 150_000], 3, 40, 29)
     bs = _arm(dev, spec)
     plan = Plan(bs, 8)
-    assert plan.blocks() >= 148
+    assert plan.blocks() >= 148 and plan.blocks() == 2 * plan.wide_blocks()
+    assert plan.batch_wide(1) and not plan.batch_wide(0)   # L = 16384 in shared mode
     plan.run_items([1, 0, 0], [2, 0, 1], [30, 5, 40])
     assert [bs[0].remaining(i) for i in range(3)] == [35, 0, 40]
     assert [bs[1].remaining(i) for i in range(3)] == [40, 40, 10]
@@ -207,3 +208,27 @@ def test_plan_run_items_lists(dev):
     for (moduli, exps, base), b in zip(spec, bs):
         for i in range(3):
             assert b.remaining(i) == 0 and b.read(i) == powm(base, exps[i], moduli[i])
+
+
+def test_wide_and_global_16384_in_one_plan(dev):
+    """L = 16384 runs as wide items (a whole block, the vector in shared memory) or, for a batch
+    tuned to global mode, on a worker in global mode; beside L = 512 items both end with the raw
+    limbs of the batches run alone, and with pow_mod."""
+    from montmul_b200.backend import Plan
+    spec = _batches(dev, [200_000, 190_000, 4000], 4, 30, 41)
+    bs = _arm(dev, spec)
+    be, st = bs[1].backend_and_state()
+    be.set_schedule(st, True, launch_steps=7)
+    plan = Plan(bs, 16)
+    assert [plan.batch_wide(i) for i in range(3)] == [True, False, False]
+    plan.run_items([2, 0, 1, 0, 2], [0, 1, 2, 3, 3], [30, 11, 30, 30, 5])
+    plan.run(30)
+    alone = _arm(dev, spec)
+    for b in alone:
+        b.run(30)
+    for (moduli, exps, base), bm, ba in zip(spec, bs, alone):
+        for i in range(4):
+            assert bm.remaining(i) == 0
+            assert bm.read_raw(i) == ba.read_raw(i), f"L {bm.params.len} slot {i}"
+            assert bm.read(i) == powm(base, exps[i], moduli[i])
+    plan.close()

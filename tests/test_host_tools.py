@@ -93,9 +93,10 @@ class _Seg:
         self.active = {s: None for s in rem}
 
 
-def _server(segs, steps, ns, blocks):
+def _server(segs, steps, ns, blocks, units=None):
     srv = serve.Server.__new__(serve.Server)
     srv.plan_segs, srv.seg_steps, srv.seg_ns, srv.blocks = segs, steps, ns, blocks
+    srv.seg_units = units or [1] * len(segs)
     return srv
 
 
@@ -103,7 +104,7 @@ def test_work_list_full_budgets_when_slots_fit():
     segs = [_Seg({0: 10_000, 1: 50}), _Seg({3: 10_000})]
     items = _server(segs, [400, 128], [700.0, 2300.0], 8).work_list()
     assert sorted((b, s, n) for b, s, n, *_ in items) == [(0, 0, 400), (0, 1, 50), (1, 3, 128)]
-    durs = [n * ns for _, _, n, _, ns in items]
+    durs = [n * ns for _, _, n, _, ns, _ in items]
     assert durs == sorted(durs, reverse=True)
 
 
@@ -113,15 +114,26 @@ def test_work_list_packs_blocks_evenly():
     w, a = 10, 14
     segs = [_Seg({s: 1_000_000 + s for s in range(a)})]
     items = _server(segs, [100], [1.0], w).work_list()
-    budgets = sorted(n for _, _, n, _, _ in items)
+    budgets = sorted(n for _, _, n, *_ in items)
     assert budgets == [50] * 8 + [100] * 6
     assert sum(budgets) == w * 100
     # longest first, so the greedy queue pairs the halves on the remaining blocks
-    assert [n for _, _, n, _, _ in items] == [100] * 6 + [50] * 8
+    assert [n for _, _, n, *_ in items] == [100] * 6 + [50] * 8
 
 
 def test_work_list_larger_shares_go_to_slots_nearest_completion():
     segs = [_Seg({0: 5_000, 1: 90_000, 2: 80_000})]
     items = _server(segs, [1000], [1.0], 2).work_list()
-    got = {s: n for _, s, n, _, _ in items}
+    got = {s: n for _, s, n, *_ in items}
     assert got[0] == 1000 and got[1] == got[2] == 500
+
+
+def test_work_list_counts_wide_items_as_two_workers():
+    """Wide items (a whole block: both workers) count two units: 2 wide + 2 other items on
+    W = 4 workers are 6 units, so the two nearest completion (the wide ones here) keep full
+    budgets and the others take half; the work fills the workers for one budget's time."""
+    segs = [_Seg({0: 1_000, 1: 2_000}), _Seg({0: 900_000, 1: 800_000})]
+    items = _server(segs, [100, 100], [1.0, 1.0], 4, units=[2, 1]).work_list()
+    got = {(b, s): n for b, s, n, *_ in items}
+    assert got == {(0, 0): 100, (0, 1): 50, (1, 0): 50, (1, 1): 50}
+    assert sum(n * (2 if b == 0 else 1) for (b, _), n in got.items()) == 4 * 100
