@@ -72,7 +72,7 @@ struct MixedDesc {
     uint32_t bits;  // steps per item of this batch in this launch (0: the launch's `bits`)
 };
 constexpr int kMixedThreads = 256;        // one group: the threads on one slot
-constexpr int kMixedGroups = 2;           // groups per block
+constexpr int kMixedGroups = 2;           // groups per block (gsync has barriers for two)
 constexpr int kMixedBlockThreads = kMixedThreads * kMixedGroups;
 constexpr int kMaxMixedSharedLogN = 12;   // 96 KiB per group, as global mode's tiles
 constexpr int kMixedGroupSmem = 24 << kMaxMixedSharedLogN;

@@ -19,22 +19,26 @@ namespace mm {
 
 // ---- thread groups ----
 // One slot is worked on by a group of NT threads (NT a power of two, a multiple of 32). A block
-// is one group (the uniform launches) or several (the mixed launch runs two groups of 256 per
-// block). Group g synchronizes on hardware barrier 1 + g with its NT threads only, so the groups
-// of a block run independently.
+// is one group (the uniform launches, and the mixed launch's wide items) or two (the mixed
+// launch's two 256-thread workers). Group 0 synchronizes on hardware barrier 1 and group 1 on
+// barrier 2, each with its NT threads only, so the two groups of a block run independently. The
+// barrier IDs are immediates: an ID held in a register made the barriers of short steps about
+// twice as slow (L = 256: 62 vs 33 ns per slot-step in the uniform launch).
 template <int NT> __device__ __forceinline__ int gtid() { return (int)(threadIdx.x & (NT - 1)); }
-template <int NT> __device__ __forceinline__ int gbar() { return 1 + (int)(threadIdx.x / NT); }
+template <int NT> __device__ __forceinline__ bool group0() { return NT >= 512 || threadIdx.x < NT; }
 template <int NT> __device__ __forceinline__ void gsync() {
-    asm volatile("bar.sync %0, %1;" ::"r"(gbar<NT>()), "n"(NT) : "memory");
+    if (group0<NT>()) asm volatile("bar.sync 1, %0;" ::"n"(NT) : "memory");
+    else asm volatile("bar.sync 2, %0;" ::"n"(NT) : "memory");
 }
 // Barrier of the group that returns whether `pred` is non-zero on any of its threads.
 template <int NT> __device__ __forceinline__ int gsync_or(int pred) {
     int r;
-    asm volatile(
-        "{ .reg .pred p, q; setp.ne.s32 p, %1, 0; bar.red.or.pred q, %2, %3, p; selp.s32 %0, 1, 0, q; }"
-        : "=r"(r)
-        : "r"(pred), "r"(gbar<NT>()), "n"(NT)
-        : "memory");
+    if (group0<NT>())
+        asm volatile("{ .reg .pred p, q; setp.ne.s32 p, %1, 0; bar.red.or.pred q, 1, %2, p; selp.s32 %0, 1, 0, q; }"
+                     : "=r"(r) : "r"(pred), "n"(NT) : "memory");
+    else
+        asm volatile("{ .reg .pred p, q; setp.ne.s32 p, %1, 0; bar.red.or.pred q, 2, %2, p; selp.s32 %0, 1, 0, q; }"
+                     : "=r"(r) : "r"(pred), "n"(NT) : "memory");
     return r;
 }
 
