@@ -93,8 +93,11 @@ struct MixedLists {
 typedef void (*MixedFn)(const MixedDesc*, MixedLists, uint32_t);
 MixedFn mixed_kernel();               // mm_mixed.cu
 
-// Threads per block for transform length 2^m: one radix-8 group per thread up to 256 threads.
-constexpr int threads_for(int m) { return m - 3 <= 5 ? 32 : (m - 3 >= 8 ? 256 : (1 << (m - 3))); }
+// Threads per block for transform length 2^m: one radix-8 group per thread up to 256 threads;
+// n = 8192 (one block per SM, all of its shared memory) takes 512, which hide more latency.
+constexpr int threads_for(int m) {
+    return m >= kWideLogN ? kWideThreads : (m - 3 <= 5 ? 32 : (m - 3 >= 8 ? 256 : (1 << (m - 3))));
+}
 
 // Defined in mm_inst.cu for each m in [kMinLogN, kMaxSharedLogN].
 #define MM_DECLARE_KERNELS(M) KernelSet kernels_m##M();
