@@ -6,9 +6,10 @@ Requests arrive as a Poisson process. Each transform length has a lane: uniform 
 admitted as soon as a slot of its length is free; a lane grows by one segment while the device
 memory budget allows (admission by the per-slot bytes of its length), else the request waits.
 Every tick is one mixed-length plan launch over a work list of every busy slot (persistent blocks
-over a device work queue, replayed from a CUDA graph). The costliest length runs `quantum` steps
-and every other length the steps that take as long (from the tuned cost per step); when busy
-slots outnumber the resident blocks, the budgets come in two sizes that pack the blocks evenly.
+over device work queues, replayed from a CUDA graph; L = 16384 slots take a whole block, the
+others one of its two workers). The slowest length runs `quantum` steps and every other length
+the steps that take as long on its worker (from the tuned cost per step); when busy slots
+outnumber the workers, the budgets come in two sizes that pack the workers evenly.
 Then the slots that finished are read back and refilled in place with waiting requests: the
 batch is never drained.
 

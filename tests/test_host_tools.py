@@ -2,6 +2,8 @@
 facts, the mixed and served workloads, the CLI's sequence and percentile helpers."""
 import math
 
+import pytest
+
 from montmul_b200 import mixed, serve, tune
 from montmul_b200.__main__ import tribonacci
 from montmul_b200.batch import Params
@@ -32,6 +34,40 @@ def test_tune_table_roundtrip(tmp_path, monkeypatch):
     assert tune.schedule_for("dev", 8192)["step_ns"] == 680.0
     assert tune.schedule_for("dev", 4096) is None
     assert tune.schedule_for("other", 8192) is None
+
+
+class _FakeDev:
+    def device_name(self):
+        return "dev"
+
+    def sm_count(self):
+        return 148
+
+
+def test_tune_mixed_only_remeasures_the_mixed_cost_and_keeps_schedules(tmp_path, monkeypatch):
+    """`tune --mixed-only` drops each listed row's mixed-launch cost and measures it again; the
+    schedule (mode, steps per launch, uniform cost) stays."""
+    monkeypatch.setenv("MONTMUL_B200_SCHEDULES", str(tmp_path / "s.json"))
+    tune.save_table({"dev": {"8192": {"global": False, "launch_steps": 64, "step_ns": 709.0, "slots": 1184,
+                                      "steps": 600, "mixed_ns": 787.0},
+                             "16384": {"global": False, "launch_steps": 512, "step_ns": 1452.0, "slots": 1184,
+                                       "steps": 300}}})
+    calls = []
+
+    def fake_mixed(dev, length, slots, steps, seed=2026):
+        calls.append((length, slots, steps))
+        return length * 1e-13
+
+    monkeypatch.setattr(tune, "measure_mixed", fake_mixed)
+    monkeypatch.setattr(tune, "tune_length", lambda *a, **k: pytest.fail("a schedule was re-tuned"))
+    tune.tune(_FakeDev(), [8192, 16384], log=lambda *_: None, mixed_only=True)
+    assert calls == [(8192, 1184, 600), (16384, 1184, 300)]
+    row = tune.schedule_for("dev", 8192)
+    assert row["mixed_ns"] == pytest.approx(8192 * 1e-4) and row["step_ns"] == 709.0 and row["launch_steps"] == 64
+    assert tune.schedule_for("dev", 16384)["mixed_ns"] == pytest.approx(16384 * 1e-4)
+    # without the flag, rows that have a mixed-launch cost keep it
+    tune.tune(_FakeDev(), [8192], log=lambda *_: None)
+    assert len(calls) == 2
 
 
 def test_mixed_workload():
