@@ -28,6 +28,10 @@ __device__ __noinline__ void mixed_wide(const SlotArgs& a, uint32_t slot, uint32
     step_slot<kWideLogN, kWideThreads>(a, slot, bits, smem, sc);
 }
 
+// gsync / gsync_or (mm_ntt.cuh) give a block at most two groups, and treat a group of 512 or
+// more threads as the whole block.
+static_assert(kMixedGroups == 2 && kWideThreads == 512, "group barriers: two workers, one wide group");
+
 constexpr int kGroupScratch = CarryScratch<kMixedThreads>::words;
 constexpr int kScratchWords = cmax(kMixedGroups * kGroupScratch, CarryScratch<kWideThreads>::words);
 
