@@ -861,6 +861,7 @@ int mm_b200_read_slots(mm_b200_batch* b, size_t count, const size_t* slots, uint
 struct mm_b200_plan {
     mm_b200_device* dev = nullptr;
     std::vector<mm_b200_batch*> batches;
+    std::vector<char> wide;           // per batch: its slots are in d_wide (its kind at creation)
     std::vector<cudaEvent_t> ready;   // per batch: its stream's work before a launch
     cudaEvent_t done = nullptr;       // the plan's last launch
     cudaStream_t stream = nullptr;
@@ -925,6 +926,16 @@ cudaError_t plan_launch(mm_b200_plan* p, const uint4* items, const uint4* wide, 
     return cudaGetLastError();
 }
 
+// Descriptor of batch i for plan_run and plan_run_each, whose item lists were built at creation:
+// a batch keeps the kind it had then. A wide batch runs in shared mode on whole blocks whatever
+// its schedule says now; any other batch of L = 16384 (tuned to global mode at creation) runs
+// in global mode on a worker, whose 96 KiB cannot hold its vector. The per-slot constants are
+// the same in both modes, so the results do not depend on the mode.
+MixedDesc plan_desc(const mm_b200_plan* p, size_t i, uint32_t bits) {
+    const mm_b200_batch* b = p->batches[i];
+    return mixed_desc(b, !p->wide[i] && (plan_global(b) || b->m == kWideLogN), bits);
+}
+
 // One launch of `bits` steps over every slot.
 int plan_enqueue(mm_b200_plan* p, uint32_t bits) {
     MM_CK(plan_launch(p, p->d_items, p->d_wide, p->d_count, bits));
@@ -956,6 +967,8 @@ int mm_b200_plan_create(mm_b200_batch* const* batches, size_t count, size_t quan
     std::unique_ptr<mm_b200_plan, void (*)(mm_b200_plan*)> p(new mm_b200_plan(), mm_b200_plan_destroy);
     p->dev = dev;
     p->batches.assign(batches, batches + count);
+    p->wide.assign(count, 0);
+    for (size_t i = 0; i < count; ++i) p->wide[i] = plan_wide(batches[i]) ? 1 : 0;
     p->quantum = quantum;
     p->count = (uint32_t)total;
     MM_CK(cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking));
@@ -984,7 +997,7 @@ int mm_b200_plan_create(mm_b200_batch* const* batches, size_t count, size_t quan
         const double c = step_cost(batches[i], plan_global(batches[i]));
         for (size_t s = 0; s < batches[i]->slots; ++s) {
             const uint4 it = make_uint4((unsigned)i, (unsigned)s, 0u, 0u);
-            if (plan_wide(batches[i])) wide.push_back(it);
+            if (p->wide[i]) wide.push_back(it);
             else items.push_back({c, it});
         }
     }
@@ -1024,7 +1037,7 @@ int mm_b200_plan_run_async(mm_b200_plan* p, size_t bits) {
     }
     // Descriptors follow the batches' buffers (exponent rows can be reallocated and restrided).
     std::vector<MixedDesc> d(nb);
-    for (size_t i = 0; i < nb; ++i) d[i] = mixed_desc(p->batches[i], plan_global(p->batches[i]), 0);
+    for (size_t i = 0; i < nb; ++i) d[i] = plan_desc(p, i, 0);
     if (std::memcmp(d.data(), p->h_descs, nb * sizeof(MixedDesc)) != 0) {
         MM_CK(cudaStreamSynchronize(p->stream));   // the pinned copy may still feed the last upload
         std::memcpy(p->h_descs, d.data(), nb * sizeof(MixedDesc));
@@ -1083,7 +1096,7 @@ int mm_b200_plan_run_each_async(mm_b200_plan* p, const size_t* steps) {
     }
     // The launch's own `bits` is 0, so a batch whose budget is 0 runs no step.
     std::vector<MixedDesc> d(nb);
-    for (size_t i = 0; i < nb; ++i) d[i] = mixed_desc(p->batches[i], plan_global(p->batches[i]), (uint32_t)steps[i]);
+    for (size_t i = 0; i < nb; ++i) d[i] = plan_desc(p, i, (uint32_t)steps[i]);
     if (std::memcmp(d.data(), p->h_descs, nb * sizeof(MixedDesc)) != 0) {
         MM_CK(cudaStreamSynchronize(p->stream));
         std::memcpy(p->h_descs, d.data(), nb * sizeof(MixedDesc));

@@ -232,3 +232,29 @@ def test_wide_and_global_16384_in_one_plan(dev):
             assert bm.read_raw(i) == ba.read_raw(i), f"L {bm.params.len} slot {i}"
             assert bm.read(i) == powm(base, exps[i], moduli[i])
     plan.close()
+
+
+def test_plan_run_after_a_schedule_switch(dev):
+    """plan.run keeps the item kinds of the plan's creation: an L = 16384 batch tuned to global
+    mode (a worker item) and one in shared mode (a wide item) both switch mode after the plan
+    exists, and both end with the raw limbs of the batches run alone, and with pow_mod."""
+    from montmul_b200.backend import Plan
+    spec = _batches(dev, [190_000, 200_000], 3, 24, 43)
+    bs = _arm(dev, spec)
+    be0, st0 = bs[0].backend_and_state()
+    be0.set_schedule(st0, True, launch_steps=7)
+    plan = Plan(bs, 16)
+    assert [plan.batch_wide(i) for i in range(2)] == [False, True]
+    be0.set_schedule(st0, False, launch_steps=7)
+    be1, st1 = bs[1].backend_and_state()
+    be1.set_schedule(st1, True, launch_steps=7)
+    plan.run(24)
+    alone = _arm(dev, spec)
+    for b in alone:
+        b.run(24)
+    for (moduli, exps, base), bm, ba in zip(spec, bs, alone):
+        for i in range(3):
+            assert bm.remaining(i) == 0
+            assert bm.read_raw(i) == ba.read_raw(i), f"L {bm.params.len} slot {i}"
+            assert bm.read(i) == powm(base, exps[i], moduli[i])
+    plan.close()
