@@ -2,6 +2,7 @@
 
     python -m montmul_b200 bench --backend b200 --bits B --slots S --steps K [--csv PATH]
     python -m montmul_b200 prp   --backend b200 --index N
+    python -m montmul_b200 fermat --backend b200 [--slots 64] [--bits 4096] [--primes 4] [--seed 2026]
     python -m montmul_b200 score --backend b200 [--slots S] [--label TEXT] [--csv PATH]
     python -m montmul_b200 sweep [--bits 1024 8192 ...] [--slots S] [--ebits 256]
     python -m montmul_b200 mixed [--slots 2000] [--lo 8192] [--hi 300000] [--ebits 1000]
@@ -85,6 +86,27 @@ def cmd_prp(a) -> int:
     return 0
 
 
+def cmd_fermat(a) -> int:
+    """The CPU-sized Fermat batch (`score.fermat_workload`: random odd moduli with seeded
+    next_prime primes among them) through the Fermat driver, every slot's value and verdict
+    checked against GMP's pow_mod."""
+    from .score import fermat_checked, fermat_workload
+    from .batch import Params
+    dev = _backend(a.backend, a.device)
+    moduli, primes = fermat_workload(a.slots, a.bits, a.primes, a.seed)
+    verdicts, _, secs = fermat_checked(dev, moduli, 3)
+    prp = [i for i, v in enumerate(verdicts) if v]
+    if prp != primes:
+        raise SystemExit(f"PRP slots {prp} differ from the planted primes {primes}")
+    steps = sum(n.bit_length() for n in moduli)   # N - 1 has as many bits as N (N odd, > 1)
+    _emit([("backend", a.backend), ("device", _device_name(dev)), ("bits", a.bits),
+           ("L", Params.for_bits(a.bits, dev.supported_lengths()).len), ("slots", a.slots),
+           ("prp", len(prp)), ("prp_slots", ";".join(map(str, prp))), ("seconds", f"{secs:.4f}"),
+           ("modsq_per_s", f"{steps / secs:.2f}"), ("fermat_tests_per_hour", f"{3600.0 * a.slots / secs:.2f}"),
+           ("checked", "every_slot_pow_mod_and_verdict")], a.csv)
+    return 0
+
+
 def tribonacci(n: int) -> int:
     """T(0) = T(1) = 0, T(2) = 1, T(n) = T(n-1) + T(n-2) + T(n-3) (montmul/src/seq.rs:6-15)."""
     a, b, c = 0, 0, 1
@@ -128,6 +150,13 @@ def main(argv=None) -> int:
     p = sub.add_parser("prp", allow_abbrev=False)
     p.add_argument("--backend", required=True)
     p.add_argument("--index", type=int, required=True)
+    p = sub.add_parser("fermat", allow_abbrev=False)
+    p.add_argument("--backend", required=True)
+    p.add_argument("--slots", type=int, default=64)
+    p.add_argument("--bits", type=int, default=4096)
+    p.add_argument("--primes", type=int, default=4)
+    p.add_argument("--seed", type=int, default=2026)
+    p.add_argument("--csv")
     p = sub.add_parser("score", allow_abbrev=False)
     p.add_argument("--backend", required=True)
     p.add_argument("--slots", type=int, default=0)
@@ -174,6 +203,8 @@ def main(argv=None) -> int:
         return cmd_prp(a)
     if a.cmd == "score":
         return cmd_score(a)
+    if a.cmd == "fermat":
+        return cmd_fermat(a)
     if a.cmd == "sweep":
         from . import sweep
         print(json.dumps(sweep.main(a)))

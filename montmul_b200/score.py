@@ -57,6 +57,55 @@ def workload(cfg: ScoreConfig):
     return moduli, [(n - 1) >> shift for n in moduli]
 
 
+def fermat_workload(slots: int = 64, bits: int = 4096, primes: int = 4, seed: int = 2026):
+    """The CPU-sized Fermat batch: `slots` random odd `bits`-bit moduli (top and bottom bits set,
+    GMP's default generator seeded `seed`, as score.rs:45-61 draws its moduli), then `primes`
+    distinct slot positions drawn from the same stream, each replaced by next_prime of a random
+    `bits`-bit start with the top bit set, so both verdicts occur. Returns (moduli, positions of
+    the primes, sorted)."""
+    if slots <= 0 or not 0 <= primes <= slots or bits < 3:
+        raise MontMulError("need slots > 0, 0 <= primes <= slots and bits >= 3")
+    rng = gmp.RandState(seed)
+    moduli = [rng.random_bits(bits) | (1 << (bits - 1)) | 1 for _ in range(slots)]
+    pos = []
+    while len(pos) < primes:
+        p = rng.random_below(slots)
+        if p not in pos:
+            pos.append(p)
+    for p in pos:
+        while True:
+            q = gmp.next_prime(rng.random_bits(bits) | (1 << (bits - 1)))
+            if q.bit_length() == bits:
+                break
+        moduli[p] = q
+    return moduli, sorted(pos)
+
+
+def fermat_checked(backend, moduli, base: int = 3, chunk: int = 1 << 16):
+    """The Fermat driver (batch.rs:187-198) with every slot checked: the value left in slot i must
+    equal pow_mod(base, N_i - 1, N_i) and its verdict must be (that value == 1). Returns
+    (verdicts, raw Montgomery values, seconds spent in run)."""
+    b = ModBatch(backend, moduli, base)
+    b.load_all([1] * b.slots())
+    b.set_exponents([m.n - 1 for m in b.moduli])
+    secs = 0.0
+    while any(b.remaining(i) > 0 for i in range(b.slots())):
+        t = time.perf_counter()
+        b.run(chunk)
+        secs += time.perf_counter() - t
+    verdicts, raws = [], []
+    for i, m in enumerate(b.moduli):
+        want = gmp.powm(base, m.n - 1, m.n)
+        if b.read(i) != want:
+            raise MontMulError(f"slot {i} disagrees with pow_mod")
+        v = b.is_one(i)
+        if v != (want == 1):
+            raise MontMulError(f"slot {i}: verdict disagrees with pow_mod")
+        verdicts.append(v)
+        raws.append(b.read_raw(i))
+    return verdicts, raws, secs
+
+
 def arm(batch: ModBatch, exps) -> None:
     """Loads 1 and the exponent into every slot (score.rs:63-69)."""
     batch.load_all([1] * len(exps))

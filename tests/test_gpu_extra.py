@@ -82,6 +82,16 @@ def test_cli_prp_t802_is_prp():
     assert "prp=true" in r.stdout
 
 
+def test_cli_fermat_batch_finds_the_planted_primes():
+    """The CPU-sized Fermat batch on the B200: 64 x 4,096-bit moduli, 4 seeded next_prime primes,
+    every value and verdict checked against pow_mod by the command itself."""
+    r = _cli("fermat", "--backend", "b200")
+    assert r.returncode == 0, r.stderr
+    f = dict(kv.split("=", 1) for kv in r.stdout.split())
+    assert f["slots"] == "64" and f["L"] == "512" and f["prp"] == "4"
+    assert f["checked"] == "every_slot_pow_mod_and_verdict"
+
+
 def test_cli_score_appends_to_csv(tmp_path):
     """tests/cli.rs:28-43"""
     path = tmp_path / "score.csv"

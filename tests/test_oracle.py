@@ -182,7 +182,7 @@ def test_wraparound_matches_full_product(o):
 
 
 def test_gmp_same_raw_as_cpu(o):
-    """tests/gmp.rs:184-187 (smaller step count)."""
+    """tests/gmp.rs:63-66 (smaller step count)."""
     common.same_raw(lambda: o.OracleBackend.gmp_backend(), lambda: o.OracleBackend.plain(), 87_914, 2, 10)
 
 

@@ -118,5 +118,5 @@ def test_unknown_backend_is_rejected():
 
 def test_help_lists_the_subcommands():
     out = _cli("--help").stdout
-    for cmd in ("bench", "prp", "score", "sweep", "mixed", "serve", "tune"):
+    for cmd in ("bench", "prp", "fermat", "score", "sweep", "mixed", "serve", "tune"):
         assert cmd in out
