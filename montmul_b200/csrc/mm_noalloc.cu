@@ -2,9 +2,8 @@
 // the caller owns, with every intermediate kept in a fixed static device array instead of
 // memory allocated per call or per batch.
 //
-// It serves callers that cannot allocate device memory when they multiply: code running under
-// CUDA stream capture (cudaMalloc and cudaFree are not capturable), services whose device
-// memory is owned by their own pool allocator and may not grow behind its back, and
+// It serves callers that cannot allocate device memory when they multiply: services whose
+// device memory is owned by their own pool allocator and may not grow behind its back, and
 // latency-critical loops that cannot afford the device-wide synchronization cudaFree implies.
 //
 // The scratch (kNoAllocScratchBytes = 256 KiB: the 2n product limbs and the n-element spectrum
@@ -129,7 +128,7 @@ extern "C" int mm_b200_mul_noalloc(const mm_b200_batch* b, size_t slot, const ui
     size_t slots = 0;
     if (!b || !d_a || !d_b || !d_out) return mm_set_error(MM_ERR_ARG, "mul_noalloc: null argument");
     if (mm_batch_plain(b)) return mm_set_error(MM_ERR_UNSUPPORTED, "mul_noalloc: needs the wraparound path (k = L/2)");
-    mm_batch_view(b, &device, &m, &c2, &c1, &tab2, &tab1, &slots);
+    if (int rc = mm_batch_view(b, &device, &m, &c2, &c1, &tab2, &tab1, &slots)) return rc;
     if (slot >= slots) return mm_set_error(MM_ERR_ARG, "mul_noalloc: bad slot");
     if (device < 0 || device >= kNoAllocMaxDevices) return mm_set_error(MM_ERR_ARG, "mul_noalloc: device ordinal too large");
     if (noalloc_bytes(m) > kNoAllocScratchBytes)
@@ -138,8 +137,20 @@ extern "C" int mm_b200_mul_noalloc(const mm_b200_batch* b, size_t slot, const ui
                                             std::to_string(kNoAllocScratchBytes));
     NoAllocFn fn = noalloc_kernel(m);
     if (!fn) return mm_set_error(MM_ERR_UNSUPPORTED, "mul_noalloc: transform length not built");
-    cudaError_t e = cudaSetDevice(device);
+    // The batch's device becomes current for the call; the caller's current device is restored
+    // on every return path.
+    int prev = 0;
+    cudaError_t e = cudaGetDevice(&prev);
     if (e != cudaSuccess) return mm_set_error(MM_ERR_CUDA, std::string("mul_noalloc: ") + cudaGetErrorString(e));
+    struct Restore {
+        int dev, cur;
+        ~Restore() { if (cur != dev) cudaSetDevice(dev); }
+    } restore{prev, prev};
+    if (device != prev) {
+        e = cudaSetDevice(device);
+        if (e != cudaSuccess) return mm_set_error(MM_ERR_CUDA, std::string("mul_noalloc: ") + cudaGetErrorString(e));
+        restore.cur = device;
+    }
     unsigned char* scratch = nullptr;
     std::string msg;
     int rc = noalloc_setup(device, &scratch, msg);

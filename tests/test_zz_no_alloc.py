@@ -1,11 +1,12 @@
 """mm_b200_mul_noalloc: the product entry point for callers that cannot allocate device memory
-when they multiply (under CUDA stream capture, inside a service whose device memory belongs to
-its own pool allocator, or in a loop that cannot take cudaFree's device synchronization).
+when they multiply (a service whose device memory belongs to its own pool allocator, or a loop
+that cannot take cudaFree's device synchronization).
 
 The test owns its device buffers (allocated here, as such a caller would have them already),
 calls the entry point twice in a row with different operands, and requires each result to equal,
-limb for limb, what the allocating entry point mm_b200_mul writes for the same operands. It
-runs last in the suite, and also passes alone in a fresh process.
+limb for limb, what the allocating entry point mm_b200_mul writes for the same operands and what
+the oracle (the reference Cpu backend with the wraparound path) computes for the same product.
+It runs last in the suite, and also passes alone in a fresh process.
 """
 import ctypes as C
 
@@ -24,7 +25,7 @@ def _device_limbs(torch, limbs):
 
 
 @pytest.mark.parametrize("bits", [1000, 87_914, 200_000])
-def test_mul_noalloc_matches_mul(bits):
+def test_mul_noalloc_matches_mul(bits, oracle):
     torch = pytest.importorskip("torch")
     from montmul_b200 import B200
     from montmul_b200.backend import lib
@@ -37,6 +38,9 @@ def test_mul_noalloc_matches_mul(bits):
     for i, v in enumerate(vals):
         batch.load(i, v)
     be, st = batch.backend_and_state()
+    ref = ModBatch(oracle.OracleBackend.wraparound(), [n, n, n, n], 3)
+    for i, v in enumerate(vals):
+        ref.load(i, v)
 
     out = torch.zeros(k, dtype=torch.int32, device="cuda")
     err = torch.full((1,), 7, dtype=torch.int32, device="cuda")
@@ -54,4 +58,6 @@ def test_mul_noalloc_matches_mul(bits):
         got = out.cpu().numpy().view(np.uint32)
         assert int(err.item()) == 0
         assert np.array_equal(got, want), f"bits {bits} operands ({a}, {b})"
+        ref.mul(3, a, b)
+        assert np.array_equal(got, to_limbs(ref.read_raw(3), k)), f"bits {bits} operands ({a}, {b}): oracle"
         assert batch.read(3) == vals[a] * vals[b] % n
