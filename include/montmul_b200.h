@@ -3,7 +3,7 @@
  *
  * The ABI mirrors the reference's backend contract, the `Limits` and `Backend` traits of
  * montmul/src/transform.rs:11-20 and 61-77, as implemented by the CUDA backend `Gpu`
- * (montmul/src/gpu/mod.rs:321-398). The caller (the host API `ModBatch`, batch.rs:130-261)
+ * (montmul/src/gpu/mod.rs:321-398). The caller (the host API `ModBatch`, batch.rs:53-184)
  * keeps the big-integer work — N' = -N^-1 mod R, Montgomery conversion, is_one — and passes
  * plain little-endian 32-bit limb arrays.
  *
@@ -13,7 +13,8 @@
  *     product that must fit, slot i");
  *   - the backend copies every input; the caller owns its buffers;
  *   - one batch is used by one host thread at a time (the trait's &mut State).
- * The wraparound path is always on (k = L/2, GpuOptions::wraparound, gpu/mod.rs:36-44).
+ * The wraparound path is on by default (k = L/2, GpuOptions::wraparound, gpu/mod.rs:36-44);
+ * mm_b200_options.wraparound = 0 selects the plain REDC with k = k0 (Cpu::default).
  */
 #ifndef MONTMUL_B200_H
 #define MONTMUL_B200_H
@@ -46,7 +47,7 @@ typedef struct mm_b200_batch mm_b200_batch;   /* `GpuState` (gpu/mod.rs:237-258)
 typedef struct {
     int device;
     int force_global;
-    int wraparound;
+    int wraparound;          /* 1 (default): k = L/2 and the wraparound REDC; 0: k = k0, plain REDC */
     int max_launch_steps;
 } mm_b200_options;
 
@@ -112,19 +113,31 @@ void *mm_b200_stream(mm_b200_batch *b);
 /* Kernel launches issued by this batch so far (for launch accounting). */
 uint64_t mm_b200_launches(const mm_b200_batch *b);
 
+/* Failure path of the bounded waits (no counterpart in the reference): every wait of a kernel on
+ * a bulk copy gives up after a time limit (100 ms in the step kernels), sets the slot's error
+ * word to 2, and the call reports MM_ERR_CUDA "... did not complete within its time limit" with
+ * the context still usable (the reference's error-word check, gpu/mod.rs:179-184). This runs
+ * that wait once on the batch's stream against an mbarrier armed for a copy that is never
+ * issued, with a limit of limit_ns (1 us .. 1 s), and returns what run would after a late copy:
+ * MM_ERR_CUDA naming slot 0. The batch's state is not changed. */
+int mm_b200_wait_check(mm_b200_batch *b, uint64_t limit_ns);
+
 /* a b R^-1 mod N (lazy, in [0, 2N)) for slot `slot`'s modulus N, without allocating: no
  * counterpart in the reference. For callers that cannot allocate device memory at the point of
- * the call: code under CUDA stream capture (cudaMalloc/cudaFree cannot be captured), services
- * whose device memory belongs to their own pool allocator, loops that cannot afford cudaFree's
- * implicit device synchronization. d_a, d_b (inputs) and d_out (output) are device buffers of k
- * limbs the caller owns; d_err (optional) receives 0, or 1 when a carry that must vanish did
- * not. The work is enqueued on `stream` (a cudaStream_t; NULL is the legacy default stream)
- * and the call returns without waiting. Intermediates live in a static 256 KiB device array
- * that every GPU loading this library holds until exit; lengths needing more scratch (the
- * global-mode lengths, L >= 32768) are rejected with MM_ERR_ARG. The first call on each
- * device looks up that array's device address and sets kernel attributes, so make it before
- * any stream capture. All calls share the array: calls that overlap on the GPU race and must
- * be serialized by the caller. */
+ * the call: services whose device memory belongs to their own pool allocator, and loops that
+ * cannot afford cudaFree's implicit device synchronization. d_a, d_b (inputs) and d_out (output)
+ * are device buffers of k limbs the caller owns; d_err (optional) receives 0, or 1 when a carry
+ * that must vanish did not. The work is enqueued on `stream` (a cudaStream_t; NULL is the
+ * legacy default stream) and the call returns without waiting. The kernel reads the slot's
+ * per-batch constants, so work still queued on the batch's own stream that writes them
+ * (mm_b200_set_moduli) must be complete first: call mm_b200_sync(b), or make `stream` wait on
+ * an event recorded on mm_b200_stream(b). The batch's device is made current for the call and
+ * the caller's current device is restored before it returns. Intermediates live in a static
+ * 256 KiB device array that every GPU loading this library holds until exit; lengths needing
+ * more scratch (the global-mode lengths, L >= 32768) are rejected with MM_ERR_ARG. The first
+ * call on each device looks up that array's device address and sets kernel attributes, so make
+ * it before any stream capture. All calls share the array: calls that overlap on the GPU race
+ * and must be serialized by the caller. */
 int mm_b200_mul_noalloc(const mm_b200_batch *b, size_t slot, const uint32_t *d_a, const uint32_t *d_b,
                         uint32_t *d_out, uint32_t *d_err, void *stream);
 

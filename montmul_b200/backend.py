@@ -62,6 +62,7 @@ SIGNATURES = {
     "mm_b200_stream": ([_vp], _vp),
     "mm_b200_launches": ([_vp], C.c_uint64),
     "mm_b200_mul_noalloc": ([_vp, _sz, _vp, _vp, _vp, _vp, _vp], C.c_int),
+    "mm_b200_wait_check": ([_vp, C.c_uint64], C.c_int),
     "mm_b200_bfly_peak": ([C.c_int, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)], C.c_int),
     "mm_b200_set_schedule": ([_vp, _vp], C.c_int),
     "mm_b200_get_schedule": ([_vp, _vp], C.c_int),
@@ -173,6 +174,7 @@ class B200:
         wraparound: GpuOptions::wraparound (gpu/mod.rs:36-44): k = L/2 and the half-length cyclic
         REDC (bit-identical to Cpu::with_wraparound); off, k = k0 and the plain REDC
         (bit-identical to Cpu::default)."""
+        self.device = device
         opts = Options(device, int(force_global), int(wraparound), max_launch_steps)
         self._tuned = tuned and not max_launch_steps and not force_global
         self._table = None
@@ -269,6 +271,11 @@ class B200:
 
     def mul(self, st, out, a, b):
         _check(lib().mm_b200_mul(st.ptr, out, a, b))
+
+    def wait_check(self, st, limit_ns: int) -> None:
+        """Runs a bulk-copy wait that is bound to run out after limit_ns on the batch's stream;
+        raises MontMulError with the time-out message, as run does after a late copy."""
+        _check(lib().mm_b200_wait_check(st.ptr, int(limit_ns)))
 
     def read(self, st, i):
         o = np.zeros(st.k, np.uint32)

@@ -60,6 +60,8 @@ struct GlobalKernels {
 };
 constexpr int kMinGlobalLogN = 12;   // smallest length the global kernels accept (one tile per half)
 GlobalKernels global_kernels();       // mm_global.cu
+// Enqueues wait_check_kernel (mm_global.cuh) on a stream; non-zero if the launch failed.
+int launch_wait_check(uint32_t* err, uint64_t limit_ns, void* stream);   // mm_global.cu
 
 // The mixed-length persistent launch (mm_mixed.cu): one descriptor per batch, one work item
 // (descriptor index, slot) per slot. Each block first takes "wide" items (L = 16384 in shared
@@ -95,8 +97,11 @@ MixedFn mixed_kernel();               // mm_mixed.cu
 
 // Threads per block for transform length 2^m: one radix-8 group per thread up to 256 threads;
 // n = 8192 (one block per SM, all of its shared memory) takes 512, which hide more latency.
+// n = 4096 takes 512 too: one radix-8 group per thread per pass, 64 registers, two blocks and 32
+// warps per SM, measured 5% faster than 256 threads with 128 registers. At the other lengths the
+// spills that 64 registers force cost more than the extra warps gain (measured 15-40% slower).
 constexpr int threads_for(int m) {
-    return m >= kWideLogN ? kWideThreads : (m - 3 <= 5 ? 32 : (m - 3 >= 8 ? 256 : (1 << (m - 3))));
+    return m >= kWideLogN || m == 12 ? 512 : (m - 3 <= 5 ? 32 : (m - 3 >= 8 ? 256 : (1 << (m - 3))));
 }
 
 // Defined in mm_inst.cu for each m in [kMinLogN, kMaxSharedLogN].

@@ -682,6 +682,14 @@ int mm_b200_mul(mm_b200_batch* b, size_t out, size_t a, size_t bb) {
     return check_err(b, "mul");
 }
 
+int mm_b200_wait_check(mm_b200_batch* b, uint64_t limit_ns) {
+    if (!b) return fail(MM_ERR_ARG, "null batch");
+    if (limit_ns < 1000 || limit_ns > 1000000000ull) return fail(MM_ERR_ARG, "wait_check: limit must be 1 us .. 1 s");
+    MM_CK(cudaSetDevice(b->dev->device));
+    if (launch_wait_check(b->d_err, limit_ns, b->stream)) return fail(MM_ERR_CUDA, "wait_check: launch failed");
+    return check_err(b, "wait_check");
+}
+
 int mm_b200_read(mm_b200_batch* b, size_t i, uint32_t* limbs) {
     if (!b || !limbs || i >= b->slots) return fail(MM_ERR_ARG, "read: bad slot");
     int rc = pull_x(b);

@@ -23,6 +23,7 @@ constexpr int kTileBytes2 = 16 * kTile, kTileBytes1 = 8 * kTile;
 constexpr int kGlobalSmem = 2 * (kTileBytes2 + kTileBytes1);   // two tile buffers: 96 KiB
 constexpr int kChunkE = 16;                                    // coefficients per thread per carry chunk
 constexpr int kErrTimeout = 2;
+constexpr uint64_t kWaitLimitNs = 100000000ull;                // bound of every wait on a bulk copy
 
 // ---- bulk copies and mbarriers (PTX) ----
 __device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -34,8 +35,9 @@ __device__ __forceinline__ void mbar_expect(uint64_t* bar, uint32_t bytes) {
     asm volatile("{ .reg .b64 st; mbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1; }" ::"r"(smem_addr(bar)), "r"(bytes)
                  : "memory");
 }
-// Waits for phase `parity` of the barrier; gives up after ~100 ms of global time.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+// Waits for phase `parity` of the barrier; gives up after about `limit_ns` of global time
+// (checked every 256 polls) or 2^26 polls, whichever comes first.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint64_t limit_ns = kWaitLimitNs) {
     const uint32_t a = smem_addr(bar);
     uint64_t t0;
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
@@ -49,7 +51,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
         if ((it & 255) == 255) {
             uint64_t t;
             asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-            if (t - t0 > 100000000ull) return false;
+            if (t - t0 > limit_ns) return false;
         }
     }
     return false;
@@ -285,7 +287,11 @@ __device__ __forceinline__ uint32_t tile_par_next(uint32_t par, int n) {
 // Runs the tile part of a transform on every tile of the n-element vector (v2, v1) in global
 // memory: full (DIF, op, DIT), DIF only, DIT only, or DIF then op (the op consumes the
 // spectrum: nothing is stored back). Returns false, the same on every thread, when a bulk copy
-// did not complete in time; no copy of this block is in flight when it returns.
+// did not complete in time. It then gives the loads of tiles c and c + 1 one more bounded wait
+// before returning, so a late copy normally lands before the block moves on; if that wait also
+// runs out (a copy stalled for over 200 ms, which no healthy GPU does), the block returns with
+// the load possibly still pending, the slot's error word reports the time-out, and the caller
+// must treat the batch's results as lost.
 template <int NT, class OP>
 __device__ __noinline__ bool tile_phase(F2* v2, F1* v1, int n, const F2K* tt2, const F1* tt1, const OP& op, int mode,
                                         const TileSmem& sm, uint32_t par) {

@@ -59,7 +59,7 @@ def radix_schedule(m: int):
 
 def threads_for(m: int) -> int:
     """Threads per block of the shared-memory kernels (mm_abi.h threads_for)."""
-    if m >= 13:
+    if m >= 12:
         return 512
     return 32 if m - 3 <= 5 else (256 if m - 3 >= 8 else 1 << (m - 3))
 

@@ -99,3 +99,26 @@ def test_global_pow_prefix(gpu):
     b.run(64)
     for i, n in enumerate(moduli):
         assert b.read(i) == powm(3, exps[i] >> (exps[i].bit_length() - 64), n)
+
+
+@pytest.mark.parametrize("bits", [300_000, 100_000])
+def test_bounded_wait_runs_out_and_context_stays_usable(gpu, wrap, bits):
+    """The failure path of the bounded waits on bulk copies (the error word of gpu/mod.rs:179-184,
+    extended with code 2): a wait on an mbarrier armed for a copy that is never issued runs out
+    after 1 ms and the call reports the time-out naming the slot, with nothing left in flight.
+    The same batch then runs normally and stays bit-exact with the oracle."""
+    rng = RandState(bits + 5)
+    moduli = [common.rand_odd(rng, bits) for _ in range(3)]
+    exps = [common.rand_exponent(rng, 24) for _ in range(3)]
+    b = ModBatch(gpu(), moduli, 3)
+    be, st = b.backend_and_state()
+    with pytest.raises(MontMulError, match="slot 0 did not complete within its time limit"):
+        be.wait_check(st, 1_000_000)
+    ref = ModBatch(wrap(), moduli, 3)
+    for batch in (b, ref):
+        batch.load_all([5, 6, 7])
+        batch.set_exponents(exps)
+        batch.run(24)
+    assert [b.read_raw(i) for i in range(3)] == [ref.read_raw(i) for i in range(3)]
+    for i, (n, e) in enumerate(zip(moduli, exps)):
+        assert b.read(i) == powm(5 + i, 1 << e.bit_length(), n) * powm(3, e, n) % n
