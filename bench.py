@@ -20,9 +20,7 @@ import argparse
 import json
 import os
 import statistics
-import subprocess
 import sys
-import tempfile
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
@@ -40,9 +38,15 @@ def g_of_n(n: int) -> int:
     return 2 * n * lg + (n // 2) * (lg - 1) + 7 * n
 
 
-# dram__bytes_read.sum + dram__bytes_write.sum of one step_kernel launch at L = 8,192 (1,184
-# slots x 16 steps): 360.3 MB + 95.6 MB, per slot-step.
-DRAM_BYTES_PER_SLOT_STEP = (360.3e6 + 95.6e6) / (1184 * 16)
+# dram__bytes_read.sum + dram__bytes_write.sum of one step_kernel launch of this workload, from
+# one ncu capture of `python -m montmul_b200.profile --slots SLOTS --steps STEPS --launches 2`
+# (second launch): the slots and steps per launch it ran, and its DRAM bytes.
+TRAFFIC_CAPTURE = {"slots": 1184, "steps_per_launch": 16, "dram_bytes": 360.3e6 + 95.6e6}
+
+# The uneven-size persistent batch: 2,000 slots, bits log-uniform in [8,192, 300,000] (seed 7),
+# c in {2, 3, 4}, the top 1,000 bits of N - 1; the plan replays its launch from a CUDA graph
+# every MIXED_QUANTUM steps.
+MIXED_SLOTS, MIXED_LO, MIXED_HI, MIXED_EBITS, MIXED_SEED, MIXED_QUANTUM = 2000, 8192, 300_000, 1000, 7, 128
 
 
 def hbm_bytes_per_slot_step(n: int) -> int:
@@ -56,68 +60,6 @@ def measured_peaks():
             return json.load(f)
     except OSError:
         return {}
-
-
-class ClockSampler:
-    """nvidia-smi clocks and throttle reasons during the timed region."""
-
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
-
-    def __init__(self, device: int):
-        self.device = device
-        self.proc = None
-        self.path = None
-
-    def __enter__(self):
-        try:
-            fd, self.path = tempfile.mkstemp(suffix=".csv")
-            os.close(fd)
-            self.out = open(self.path, "w")
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
-                                         stdout=self.out, stderr=subprocess.DEVNULL)
-        except (OSError, FileNotFoundError):
-            self.proc = None
-        return self
-
-    def __exit__(self, *exc):
-        if self.proc is not None:
-            self.proc.terminate()
-            try:
-                self.proc.wait(timeout=5)
-            except subprocess.TimeoutExpired:
-                self.proc.kill()
-            self.out.close()
-
-    def summary(self):
-        if self.proc is None or not self.path:
-            return None
-        rows = []
-        with open(self.path) as f:
-            for line in f:
-                parts = [p.strip() for p in line.split(",")]
-                if len(parts) >= 9:
-                    rows.append(parts)
-        os.unlink(self.path)
-        if not rows:
-            return None
-        def num(v):
-            try:
-                return float(v)
-            except ValueError:
-                return None
-        sm = [num(r[1]) for r in rows if num(r[1]) is not None]
-        mx = [num(r[2]) for r in rows if num(r[2]) is not None]
-        reasons = set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for r in rows:
-            for name, v in zip(names, r[5:9]):
-                if v.lower().startswith("active"):
-                    reasons.add(name)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": sorted(reasons), "samples": len(rows)}
 
 
 def dist_backend() -> str:
@@ -170,55 +112,132 @@ def barrier(world: int):
         dist.barrier()
 
 
-def cpu_baseline(seconds: float = 12.0, threads: int = 0):
-    """The reference's Cpu backend (wraparound on), restated in C, on every host core, on a
-    bounded sample of the score workload: one slot per thread, as many steps as fit ~`seconds`."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle
-    from montmul_b200 import ModBatch
-    from montmul_b200.score import ScoreConfig, arm, workload
-    oracle.build()
-    cores = threads or os.cpu_count() or 1
-    moduli, exps = workload(ScoreConfig(bits=BITS, slots=cores, ebits=EBITS, repeats=1, seed=SEED))
-    b = ModBatch(oracle.OracleBackend.wraparound(threads=cores), moduli, 3)
-    arm(b, exps)
-    t = time.perf_counter()
-    b.run(2)
-    probe = time.perf_counter() - t
-    steps = max(2, min(EBITS, int(seconds / max(probe / 2, 1e-6))))
-    arm(b, exps)
-    t = time.perf_counter()
-    b.run(steps)
-    dt = time.perf_counter() - t
-    return {"value": cores * steps / dt, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"{cores} slots x {steps} steps of the 100,000-bit score workload (L=8192), "
-                      f"{dt:.1f} s, oracle = reference Cpu backend with wraparound restated in C"}
+class CpuScore:
+    """The reference's score protocol (montmul/src/score.rs:91-136, main.rs:201-216) on one of its
+    CPU backends, restated by the oracle: `cpu` = Cpu with the wraparound path (the semantics
+    authority), `gmp` = the Gmp backend's REDC over libgmp. The slot count is the best of
+    cores x {1, 2} at 200 exponent bits (best_slots), one worker thread per core; each repeat
+    then loads 1 and the top 2,000 bits of N - 1 into every slot and runs all 2,000 steps."""
+
+    def __init__(self, kind: str, cores: int = 0):
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle
+        from montmul_b200 import ModBatch
+        from montmul_b200.score import ScoreConfig, arm, workload
+        oracle.build()
+        self.kind = kind
+        self.cores = cores or os.cpu_count() or 1
+        make = oracle.OracleBackend.wraparound if kind == "cpu" else oracle.OracleBackend.gmp_backend
+        self._arm = arm
+        best = None
+        for slots in (self.cores, 2 * self.cores):
+            moduli, exps = workload(ScoreConfig(bits=BITS, slots=slots, ebits=EBITS, repeats=1, seed=SEED))
+            probe = [(n - 1) >> (BITS - 200) for n in moduli]
+            b = ModBatch(make(threads=self.cores), moduli, 3)
+            arm(b, probe)
+            t = time.perf_counter()
+            b.run(200)
+            rate = slots * 200 / (time.perf_counter() - t)
+            if best is None or rate > best[0]:
+                best = (rate, slots, b, moduli, exps)
+        _, self.slots, self.batch, self.moduli, self.exps = best
+
+    def repeat(self):
+        """One timed repeat: (modsq/s, seconds)."""
+        self._arm(self.batch, self.exps)
+        t = time.perf_counter()
+        self.batch.run(EBITS)
+        dt = time.perf_counter() - t
+        return self.slots * EBITS / dt, dt
+
+    def check(self):
+        """Slot 0 and the last slot against GMP's pow_mod (the reference's score gate)."""
+        from montmul_b200.gmp import powm
+        for i in (0, self.slots - 1):
+            if self.batch.read(i) != powm(3, self.exps[i], self.moduli[i]):
+                raise SystemExit(f"{self.kind} baseline: slot {i} disagrees with pow_mod")
+
+    def describe(self, value, seconds, repeats):
+        name = ("reference Cpu backend (wraparound on) restated in C" if self.kind == "cpu"
+                else "reference Gmp backend (textbook REDC, k = k0) restated in C over libgmp")
+        return {"value": value, "unit": UNIT, "cores": self.cores, "kind": "port",
+                "sample": f"{self.slots} slots (best of {self.cores} x {{1,2}} host threads' slot rule) x "
+                          f"{EBITS} steps of the 100,000-bit score workload per repeat, {seconds:.1f} s per repeat, "
+                          f"median of {repeats}; {name}"}
+
+
+def cpu_baselines():
+    """Both CPU backends of the reference on this host's cores, one full repeat each."""
+    out = {}
+    for kind in ("cpu", "gmp"):
+        s = CpuScore(kind)
+        value, dt = s.repeat()
+        s.check()
+        out[kind] = s.describe(value, dt, 1)
+    return out
 
 
 def run_reference(args, world, rank):
-    """--impl reference: the reference's CPU implementation of the path (its Rust crate cannot be
-    built here, so the C restatement of its Cpu backend) on all host cores, same metric."""
+    """--impl reference: the reference's own CPU implementation of the path on all host cores,
+    same workload and metric. Its Rust crate cannot be built here, so its two CPU backends run as
+    the oracle's C restatements (Cpu, and Gmp over libgmp); the faster one on this host is the
+    reference arm. One step = one repeat of the score (2,000 steps on every slot)."""
     if rank != 0:
         return 0
-    cores = os.cpu_count() or 1
-    steps = []
-    base = None
+    arms = {kind: CpuScore(kind) for kind in ("cpu", "gmp")}
+    probe = {kind: s.repeat() for kind, s in arms.items()}
+    kind = max(probe, key=lambda k: probe[k][0])
+    s = arms[kind]
+    rates, secs = [], []
     for i in range(args.warmup + args.steps):
-        r = cpu_baseline(seconds=args.ref_seconds, threads=cores)
+        r, dt = s.repeat()
         if i >= args.warmup:
-            steps.append(r["value"])
-        base = r
-    value = statistics.median(steps)
+            rates.append(r)
+            secs.append(dt)
+    s.check()
+    value = statistics.median(rates)
+    other = "gmp" if kind == "cpu" else "cpu"
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * args.ref_seconds,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * statistics.median(secs),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
             "data": "synthetic (GMP-seeded random odd moduli, seed 2026)",
             "config": {"workload": "score: 100,000-bit odd moduli, L=8192, k=4096, base 3, top 2,000 bits of N-1",
-                       "bits": BITS, "ebits": EBITS, "L": 8192},
-            "cpu_baseline": {**base, "value": value},
+                       "bits": BITS, "ebits": EBITS, "L": 8192, "slots": s.slots, "backend": kind},
+            "cpu_baseline": s.describe(value, statistics.median(secs), args.steps),
+            "cpu_baseline_other": arms[other].describe(probe[other][0], probe[other][1], 1) | {"backend": other},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0
+
+
+def mixed_leg(device: int) -> dict:
+    """The uneven-size persistent batch (one plan over every slot, its launch replayed from a CUDA
+    graph) against the same slots run as separate uniform batches one after another, on the same
+    GPU; each timed with the host clock around the synchronous call, clocks sampled meanwhile,
+    and every slot checked against GMP's pow_mod after each run."""
+    from montmul_b200 import mixed as mx
+    from montmul_b200.backend import B200
+    from montmul_b200.clocks import ClockSampler
+    dev = B200(device=device)
+    work = mx.workload(MIXED_SLOTS, MIXED_LO, MIXED_HI, MIXED_EBITS, MIXED_SEED)
+    groups = mx.group(dev, work)
+    total = len(work) * MIXED_EBITS
+    mx.run_mixed(groups, 32, MIXED_QUANTUM)
+    mx.run_separate(groups, 32)
+    with ClockSampler(device) as c1:
+        t_sep = mx.run_separate(groups, MIXED_EBITS)
+    checked_sep = mx.verify(groups, work)
+    with ClockSampler(device) as c2:
+        t_mix, launches, graph = mx.run_mixed(groups, MIXED_EBITS, MIXED_QUANTUM)
+    checked_mix = mx.verify(groups, work)
+    return {"workload": f"{len(work)} slots, bits log-uniform in [{MIXED_LO}, {MIXED_HI}] (seed {MIXED_SEED}), "
+                        f"c in {{2,3,4}}, top {MIXED_EBITS} bits of N-1",
+            "groups": len(groups), "value": total / t_mix, "unit": UNIT,
+            "separate_value": total / t_sep, "mixed_over_separate": t_sep / t_mix,
+            "mixed_seconds": t_mix, "separate_seconds": t_sep, "launches": launches, "graph_launches": graph,
+            "quantum": MIXED_QUANTUM, "timing": "host clock around synchronous calls",
+            "clocks": c2.summary(), "clocks_separate": c1.summary(),
+            "checked": f"all {checked_mix} slots equal GMP pow_mod after the mixed run, {checked_sep} after the separate run"}
 
 
 def main(argv=None):
@@ -229,7 +248,7 @@ def main(argv=None):
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--slots", type=int, default=0, help="slots per GPU (0: best of 148 x {1,2,4,8,16})")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--ref-seconds", type=float, default=10.0)
+    ap.add_argument("--no-mixed", action="store_true", help="skip the uneven-size persistent batch leg")
     args = ap.parse_args(argv)
     if args.warmup < 3:
         ap.error("at least 3 warm-up steps")
@@ -238,11 +257,10 @@ def main(argv=None):
         return run_reference(args, int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")))
     world, rank, local = dist_init()
 
-    import ctypes as C
-
     from montmul_b200 import B200, ModBatch
     from montmul_b200 import backend as bk
     from montmul_b200.batch import exponent_words
+    from montmul_b200.clocks import ClockSampler
     from montmul_b200.gmp import powm
     from montmul_b200.score import ScoreConfig, arm, checked_slots, workload
 
@@ -299,7 +317,6 @@ def main(argv=None):
     batch = make_batch(slots)
     exps = exps_all[:slots]
     be, st = batch.backend_and_state()
-    stream = torch.cuda.ExternalStream(be.stream(st))
     arm(batch, exps)
     batch.run(64)
     for _ in range(args.warmup):
@@ -354,15 +371,21 @@ def main(argv=None):
     peaks = measured_peaks()
     hbm = peaks.get("hbm_gbs")
     achieved_gbs = slots * EBITS * hbm_bytes_per_slot_step(n) / per_step_s / 1e9
-    # DRAM traffic of one step-kernel launch: bytes per slot-step from the committed ncu capture
-    # of this kernel on this workload, times the slot-steps of one launch here.
+    # DRAM traffic of one step-kernel launch, from the committed ncu capture of this kernel on this
+    # workload; scaled by the slot-steps per launch when this run's launches differ from the
+    # captured one (the per-slot constants are re-read from L2 less often in longer launches, so
+    # the scaled figure is an estimate and says so).
     steps_per_launch = EBITS * args.steps / max(1, launches)
-    traffic = DRAM_BYTES_PER_SLOT_STEP * slots * steps_per_launch
+    cap = TRAFFIC_CAPTURE
+    same = cap["slots"] == slots and abs(cap["steps_per_launch"] - steps_per_launch) < 0.5
+    traffic = cap["dram_bytes"] * (1.0 if same else slots * steps_per_launch / (cap["slots"] * cap["steps_per_launch"]))
     roofline = {"bound": "int", "achieved": achieved_pairs / 1e9, "peak": peak_pairs / 1e9, "unit": "Gbfly/s",
                 "frac": achieved_pairs / peak_pairs, "traffic": traffic,
-                "traffic_note": "bytes per launch: %.0f B per slot-step (dram__bytes_read+write of one ncu capture, "
-                                "profiles/step_kernel_score_L8192.md) x %d slots x %.0f steps per launch"
-                                % (DRAM_BYTES_PER_SLOT_STEP, slots, steps_per_launch),
+                "traffic_note": ("dram__bytes_read+write per launch, measured by ncu on a launch of this size"
+                                 if same else
+                                 "dram__bytes_read+write of an ncu capture of %d slots x %d steps per launch, "
+                                 "scaled to this run's %d slots x %.0f steps per launch (estimate)"
+                                 % (cap["slots"], cap["steps_per_launch"], slots, steps_per_launch)),
                 "note": "butterfly pairs (GF(p^2) product + add + sub in both fields), G(n)=%d per modsq at "
                         "L=8192; peak = the kernels' own arithmetic in register-resident chains on all SMs, "
                         "measured in this run" % g_of_n(n)}
@@ -379,11 +402,15 @@ def main(argv=None):
             "fermat_tests_per_hour": value * 3600.0 / BITS, "e2e": e2e, "roofline": roofline,
             "roofline_hbm": roofline_hbm, "gpu_launches": launches, "clocks": clocks,
             "checked": "slot 0, last and 2 seeded slots equal GMP pow_mod"}
+    del batch, st
+    if world == 1 and not args.no_mixed:
+        line["mixed"] = mixed_leg(local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline()
+        base = cpu_baselines()
+        line["cpu_baseline"] = base["cpu"]
+        line["cpu_baseline_gmp"] = base["gmp"]
     if rank == 0:
         print(json.dumps(line))
-    del batch, st
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()

@@ -3,7 +3,7 @@
     python -m montmul_b200 bench --backend b200 --bits B --slots S --steps K [--csv PATH]
     python -m montmul_b200 prp   --backend b200 --index N
     python -m montmul_b200 fermat --backend b200 [--slots 64] [--bits 4096] [--primes 4] [--seed 2026]
-    python -m montmul_b200 score --backend b200 [--slots S] [--label TEXT] [--csv PATH]
+    python -m montmul_b200 score --backend b200 [--slots S] [--label TEXT] [--csv PATH] [--ncu]
     python -m montmul_b200 sweep [--bits 1024 8192 ...] [--slots S] [--ebits 256]
     python -m montmul_b200 mixed [--slots 2000] [--lo 8192] [--hi 300000] [--ebits 1000]
     python -m montmul_b200 serve [--load 0.7 0.95] [--duration 40] [--lo 10000] [--hi 200000]
@@ -115,6 +115,64 @@ def tribonacci(n: int) -> int:
     return a
 
 
+NCU_SM = "sm__throughput.avg.pct_of_peak_sustained_elapsed"
+NCU_MEM = "gpu__compute_memory_throughput.avg.pct_of_peak_sustained_elapsed"
+NCU_MAX_SLOTS_PER_SM = 2
+
+
+def parse_ncu_csv(text: str):
+    """(SM throughput %, memory throughput %) of the last profiled launch in ncu's --csv output
+    (main.rs:221-245): rows are quoted, the header names "Metric Name" and "Metric Value"."""
+    import csv
+    import io
+    rows = [r for r in csv.reader(io.StringIO("\n".join(l for l in text.splitlines() if l.startswith('"'))))]
+    if not rows:
+        raise ValueError("no ncu output")
+    head = rows[0]
+    try:
+        name, value = head.index("Metric Name"), head.index("Metric Value")
+    except ValueError as e:
+        raise ValueError(f"ncu column missing: {e}") from None
+
+    def last(metric):
+        for r in reversed(rows[1:]):
+            if len(r) > max(name, value) and r[name] == metric:
+                return float(r[value].replace(",", ""))
+        raise ValueError(f"ncu metric {metric} missing")
+
+    return last(NCU_SM), last(NCU_MEM)
+
+
+def ncu_metrics(slots: int, device: int):
+    """One 16-step launch of the score workload under Nsight Compute (clocks left alone), after
+    the same command has run once without it; returns (SM %, memory %) of that launch."""
+    import shutil
+    import subprocess
+    cmd = [sys.executable, "-m", "montmul_b200", "ncu-launch", "--slots", str(slots), "--device", str(device)]
+    plain = subprocess.run(cmd, capture_output=True, text=True, timeout=600)
+    if plain.returncode != 0:
+        raise RuntimeError(f"ncu-launch failed without ncu: {plain.stderr.strip()[-400:]}")
+    ncu = shutil.which("ncu") or "/usr/local/cuda/bin/ncu"
+    r = subprocess.run([ncu, "--csv", "--clock-control", "none", "--kernel-name", "regex:step_kernel", "-c", "1",
+                        "--metrics", f"{NCU_SM},{NCU_MEM}", *cmd], capture_output=True, text=True, timeout=900)
+    if r.returncode != 0:
+        raise RuntimeError(f"ncu failed: {r.stderr.strip()[-400:]}")
+    return parse_ncu_csv(r.stdout)
+
+
+def cmd_ncu_launch(a) -> int:
+    """The profiled launch of score --ncu (main.rs:333-342): the score workload at --slots slots,
+    armed, then one launch of 16 steps."""
+    from .backend import B200
+    from .batch import ModBatch
+    from .score import ScoreConfig, arm, workload
+    moduli, exps = workload(ScoreConfig.standard(a.slots))
+    b = ModBatch(B200(device=a.device, max_launch_steps=16), moduli, 3)
+    arm(b, exps)
+    b.run(16)
+    return 0
+
+
 def cmd_score(a) -> int:
     """The standard score at --slots, or at the best of SMs x {1, 2, 4, 8, 16} (main.rs:192-299)."""
     from .score import GMP_M5_SECONDS_PER_MODSQ_100K, ScoreConfig, best_slots, gpu_overhead, score
@@ -129,11 +187,20 @@ def cmd_score(a) -> int:
         slots = best_slots(make, 100_000, cands)
     s = score(make, ScoreConfig.standard(slots))
     s.overhead = gpu_overhead(make, ScoreConfig.standard(slots))
+    sm_pct = mem_pct = ""
+    if a.ncu:
+        # One launch on at most two slots per SM: a profile of a few milliseconds.
+        per = min(slots, NCU_MAX_SLOTS_PER_SM * dev.sm_count())
+        try:
+            sm, mem = ncu_metrics(per, a.device)
+            sm_pct, mem_pct = f"{sm:.4f}", f"{mem:.4f}"
+        except (RuntimeError, ValueError, OSError) as e:
+            print(f"warning: ncu profile failed, sm_pct and mem_pct left empty: {e}", file=sys.stderr)
     _emit([("timestamp", int(time.time())), ("label", '"' + a.label.replace('"', '""') + '"'),
            ("device", _device_name(dev)), ("backend", a.backend), ("slots", s.slots),
            ("modsq_per_s", f"{s.modsq_per_s:.2f}"), ("mad", f"{s.mad:.2f}"),
-           ("fermat_tests_per_hour", f"{s.fermat_tests_per_hour:.4f}"), ("overhead", f"{s.overhead:.4f}"), ("sm_pct", ""),
-           ("mem_pct", ""), ("gmp_core_equiv", f"{s.modsq_per_s * GMP_M5_SECONDS_PER_MODSQ_100K:.4f}")], a.csv)
+           ("fermat_tests_per_hour", f"{s.fermat_tests_per_hour:.4f}"), ("overhead", f"{s.overhead:.4f}"), ("sm_pct", sm_pct),
+           ("mem_pct", mem_pct), ("gmp_core_equiv", f"{s.modsq_per_s * GMP_M5_SECONDS_PER_MODSQ_100K:.4f}")], a.csv)
     return 0
 
 
@@ -162,6 +229,9 @@ def main(argv=None) -> int:
     p.add_argument("--slots", type=int, default=0)
     p.add_argument("--label", default="")
     p.add_argument("--csv")
+    p.add_argument("--ncu", action="store_true", help="profile one step launch with Nsight Compute")
+    p = sub.add_parser("ncu-launch", allow_abbrev=False, help=argparse.SUPPRESS)
+    p.add_argument("--slots", type=int, required=True)
     p = sub.add_parser("sweep", allow_abbrev=False)
     p.add_argument("--bits", type=int, nargs="*", default=[1024, 8192, 32768, 100_000, 300_000, 1_000_000])
     p.add_argument("--slots", type=int, default=0, help="slots per size (0: 80%% of free memory, at most --max-slots)")
@@ -173,7 +243,7 @@ def main(argv=None) -> int:
     p.add_argument("--hi", type=int, default=300_000)
     p.add_argument("--ebits", type=int, default=1000)
     p.add_argument("--seed", type=int, default=7)
-    p.add_argument("--quantum", type=int, default=1 << 16)
+    p.add_argument("--quantum", type=int, default=128, help="steps per graph-replayed launch")
     p = sub.add_parser("serve", allow_abbrev=False)
     p.add_argument("--load", type=float, nargs="*", default=[0.7, 0.95])
     p.add_argument("--duration", type=float, default=40.0, help="seconds of arrivals")
@@ -205,6 +275,8 @@ def main(argv=None) -> int:
         return cmd_score(a)
     if a.cmd == "fermat":
         return cmd_fermat(a)
+    if a.cmd == "ncu-launch":
+        return cmd_ncu_launch(a)
     if a.cmd == "sweep":
         from . import sweep
         print(json.dumps(sweep.main(a)))

@@ -118,9 +118,12 @@ def main(args) -> dict:
     # Warm-up of both paths (tables, graph capture, clocks).
     run_mixed(groups, min(args.ebits, 32), args.quantum)
     run_separate(groups, min(args.ebits, 32))
-    t_sep = run_separate(groups, args.ebits)
+    from .clocks import ClockSampler
+    with ClockSampler(args.device) as c_sep:
+        t_sep = run_separate(groups, args.ebits)
     checked_sep = verify(groups, work)
-    t_mix, launches, graph = run_mixed(groups, args.ebits, args.quantum)
+    with ClockSampler(args.device) as c_mix:
+        t_mix, launches, graph = run_mixed(groups, args.ebits, args.quantum)
     checked_mix = verify(groups, work)
     return {
         "workload": f"{len(work)} slots, bits log-uniform in [{args.lo}, {args.hi}] (seed {args.seed}), "
@@ -130,4 +133,5 @@ def main(args) -> dict:
         "mixed_over_separate": t_sep / t_mix, "mixed_seconds": t_mix, "separate_seconds": t_sep,
         "mixed_launches": launches, "mixed_graph_launches": graph, "quantum": args.quantum,
         "checked": f"all {checked_mix} slots equal GMP pow_mod after each run ({checked_sep} separate)",
+        "clocks": c_mix.summary(), "clocks_separate": c_sep.summary(),
     }

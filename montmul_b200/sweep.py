@@ -47,9 +47,11 @@ def one_size(dev, bits: int, slots: int, ebits: int, seed: int = 2026) -> dict:
     b.set_exponents(exps)
     be, st = b.backend_and_state()
     be.push(st)
-    t = time.perf_counter()
-    b.run(e_bits)
-    secs = time.perf_counter() - t
+    from .clocks import ClockSampler
+    with ClockSampler(dev.device) as clk:
+        t = time.perf_counter()
+        b.run(e_bits)
+        secs = time.perf_counter() - t
     srng = gmp.RandState(seed + 1)
     for i in [0, slots - 1] + [srng.random_below(slots) for _ in range(2)]:
         if b.read(i) != gmp.powm(3, exps[i], moduli[i]):
@@ -67,7 +69,8 @@ def one_size(dev, bits: int, slots: int, ebits: int, seed: int = 2026) -> dict:
     rate = slots * e_bits / secs
     return {"bits": bits, "L": length, "slots": slots, "ebits": e_bits, "seconds": secs, "modsq_per_s": rate,
             "bitsteps_per_s": rate * bits, "gbfly_per_s": rate * butterfly_pairs(n) / 1e9,
-            "mode": "global" if sched["global"] else "shared", "tuned": tuned, "mul_checked": muls}
+            "mode": "global" if sched["global"] else "shared", "tuned": tuned, "mul_checked": muls,
+            "clocks": clk.summary()}
 
 
 def main(args) -> dict:

@@ -120,3 +120,27 @@ def test_help_lists_the_subcommands():
     out = _cli("--help").stdout
     for cmd in ("bench", "prp", "fermat", "score", "sweep", "mixed", "serve", "tune"):
         assert cmd in out
+
+
+NCU_SAMPLE = '''==PROF== Connected to process 4242 (/usr/bin/python3.12)
+==PROF== Profiling "step_kernel": 0%....50%....100% - 1 pass
+"ID","Process ID","Process Name","Host Name","Kernel Name","Context","Stream","Block Size","Grid Size","Device","CC","Section Name","Metric Name","Metric Unit","Metric Value"
+"0","4242","python3.12","127.0.0.1","void mm::step_kernel<12, 256>(mm::SlotArgs, unsigned int, unsigned int)","1","13","(256, 1, 1)","(296, 1, 1)","0","10.0","Command line profiler metrics","gpu__compute_memory_throughput.avg.pct_of_peak_sustained_elapsed","%","1,234.5"
+"0","4242","python3.12","127.0.0.1","void mm::step_kernel<12, 256>(mm::SlotArgs, unsigned int, unsigned int)","1","13","(256, 1, 1)","(296, 1, 1)","0","10.0","Command line profiler metrics","sm__throughput.avg.pct_of_peak_sustained_elapsed","%","56.78"
+==PROF== Disconnected from process 4242
+'''
+
+
+def test_ncu_csv_parser_reads_the_last_launch():
+    """main.rs:221-245: quoted rows, "Metric Name"/"Metric Value" columns, thousands separators."""
+    from montmul_b200.__main__ import parse_ncu_csv
+    assert parse_ncu_csv(NCU_SAMPLE) == (56.78, 1234.5)
+    two = NCU_SAMPLE + NCU_SAMPLE.splitlines()[4].replace('"56.78"', '"60.5"') + "\n"
+    assert parse_ncu_csv(two)[0] == 60.5
+
+
+@pytest.mark.parametrize("text", ["", "==PROF== nothing\n", '"A","B"\n"1","2"\n'])
+def test_ncu_csv_parser_rejects_missing_output(text):
+    from montmul_b200.__main__ import parse_ncu_csv
+    with pytest.raises(ValueError):
+        parse_ncu_csv(text)
