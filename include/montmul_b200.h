@@ -113,6 +113,15 @@ void *mm_b200_stream(mm_b200_batch *b);
 /* Kernel launches issued by this batch so far (for launch accounting). */
 uint64_t mm_b200_launches(const mm_b200_batch *b);
 
+/* Serving launches (no counterpart in the reference): run_items_async enqueues, on the batch's
+ * stream, one launch of the uniform step kernel over an explicit list, slot slots[i] running up
+ * to steps[i] steps (each slot at most once, steps[i] >= 1), and returns; mm_b200_sync waits and
+ * reports errors as run does. Lists of several batches on their own streams run on the device
+ * at the same time. Shared-memory lengths only (L <= 16384). blocks_per_sm: blocks of the
+ * batch's step kernel that one SM holds at once (0 on an error). */
+int mm_b200_run_items_async(mm_b200_batch *b, size_t count, const size_t *slots, const uint32_t *steps);
+int mm_b200_blocks_per_sm(const mm_b200_batch *b);
+
 /* Failure path of the bounded waits (no counterpart in the reference): every wait of a kernel on
  * a bulk copy gives up after a time limit (100 ms in the step kernels), sets the slot's error
  * word to 2, and the call reports MM_ERR_CUDA "... did not complete within its time limit" with

@@ -63,6 +63,8 @@ SIGNATURES = {
     "mm_b200_launches": ([_vp], C.c_uint64),
     "mm_b200_mul_noalloc": ([_vp, _sz, _vp, _vp, _vp, _vp, _vp], C.c_int),
     "mm_b200_wait_check": ([_vp, C.c_uint64], C.c_int),
+    "mm_b200_run_items_async": ([_vp, _sz, _vp, _vp], C.c_int),
+    "mm_b200_blocks_per_sm": ([_vp], C.c_int),
     "mm_b200_bfly_peak": ([C.c_int, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)], C.c_int),
     "mm_b200_set_schedule": ([_vp, _vp], C.c_int),
     "mm_b200_get_schedule": ([_vp, _vp], C.c_int),
@@ -272,6 +274,18 @@ class B200:
     def mul(self, st, out, a, b):
         _check(lib().mm_b200_mul(st.ptr, out, a, b))
 
+    def run_items_async(self, st, slots, steps) -> None:
+        """One launch over a list: slot slots[i] runs up to steps[i] steps (each slot once);
+        returns at once, sync() waits and checks errors."""
+        s = np.ascontiguousarray(slots, np.uintp)
+        t = np.ascontiguousarray(steps, np.uint32)
+        assert s.size == t.size
+        _check(lib().mm_b200_run_items_async(st.ptr, s.size, _ptr(s), _ptr(t)))
+
+    def blocks_per_sm(self, st) -> int:
+        """Blocks of the batch's step kernel one SM holds at once."""
+        return int(lib().mm_b200_blocks_per_sm(st.ptr))
+
     def wait_check(self, st, limit_ns: int) -> None:
         """Runs a bulk-copy wait that is bound to run out after limit_ns on the batch's stream;
         raises MontMulError with the time-out message, as run does after a late copy."""
@@ -340,14 +354,18 @@ class B200:
         return TBuf(ptr, length, count, self)
 
     # Schedules and in-place refill (no counterpart in the reference's Backend trait).
-    def set_schedule(self, st, global_mode: bool, launch_steps: int = 0, step_ns: float = 0.0):
+    def set_schedule(self, st, global_mode, launch_steps: int = 0, step_ns: float = 0.0):
+        """global_mode: 0 (or False) shared memory, 1 (or True) global mode, 2 cluster mode
+        (L = 32768 and 65536: one thread-block cluster per slot, the vector in the cluster's
+        shared memory)."""
         sc = Schedule(int(global_mode), int(launch_steps), float(step_ns))
         _check(lib().mm_b200_set_schedule(st.ptr, C.byref(sc)))
 
     def get_schedule(self, st):
         sc = Schedule()
         _check(lib().mm_b200_get_schedule(st.ptr, C.byref(sc)))
-        return {"global": bool(sc.global_), "launch_steps": sc.launch_steps, "step_ns": sc.step_ns}
+        return {"global": bool(sc.global_), "mode": ("shared", "global", "cluster")[sc.global_],
+                "launch_steps": sc.launch_steps, "step_ns": sc.step_ns}
 
     def set_moduli(self, st, slots, n, nprime):
         ids = np.ascontiguousarray(slots, np.uintp)

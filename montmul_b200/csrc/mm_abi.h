@@ -2,6 +2,8 @@
 // instantiations (mm_inst.cu, compiled once per log2 n): the kernel argument block and the
 // table of kernel entry points of one length.
 #pragma once
+#include <vector_types.h>
+
 #include "mm_common.h"
 
 namespace mm {
@@ -25,7 +27,7 @@ struct SlotArgs {
     uint32_t plain;       // 1: REDC without the wraparound path (constants F(N') | F(N))
 };
 
-typedef void (*StepFn)(SlotArgs, uint32_t, uint32_t);
+typedef void (*StepFn)(SlotArgs, uint32_t, uint32_t, const uint2*);
 typedef void (*MulFn)(SlotArgs, uint32_t, uint32_t, uint32_t, F2*, F1*);
 typedef void (*SetupFn)(const uint32_t*, const uint32_t*, F2*, F1*, const F2K*, const F1*, F2, F1, uint32_t,
                         const uint32_t*, uint32_t, int);
@@ -60,6 +62,13 @@ struct GlobalKernels {
 };
 constexpr int kMinGlobalLogN = 12;   // smallest length the global kernels accept (one tile per half)
 GlobalKernels global_kernels();       // mm_global.cu
+// Cluster mode (mm_cluster.cu): L = 32768 and 65536, one thread-block cluster of n / 8192
+// blocks per slot. cluster_configure sets the kernels' shared-memory opt-in on the current
+// device; cluster_launch runs `bits` steps on every slot of a batch.
+constexpr int kMinClusterLogN = 14;
+constexpr int kMaxClusterLogN = 15;
+int cluster_configure();
+int cluster_launch(int m, const SlotArgs& a, uint32_t slots, uint32_t bits, void* stream);
 // Enqueues wait_check_kernel (mm_global.cuh) on a stream; non-zero if the launch failed.
 int launch_wait_check(uint32_t* err, uint64_t limit_ns, void* stream);   // mm_global.cu
 

@@ -75,6 +75,7 @@ struct mm_b200_device {
     bool wrap = true;          // GpuOptions::wraparound (k = L/2); off: k = k0 and the plain REDC
     bool global_configured = false;
     bool mixed_configured = false;
+    bool cluster_configured = false;
     std::string name;
     std::mutex mu;
     std::map<int, DevTables> tables;
@@ -88,6 +89,8 @@ struct mm_b200_batch {
     uint32_t base = 3;
     KernelSet ks{};
     bool global = false;       // vector in HBM, tiles through shared memory (mm_global.cuh)
+    bool cluster = false;      // global batch stepped in cluster mode (mm_cluster.cuh)
+    const DevTables* ctab = nullptr;   // shared-layout tables of a cluster-mode length
     bool plain = false;        // REDC without the wraparound path (k may be below L/2)
     GlobalKernels gk{};
     F2* d_w2 = nullptr;        // global mode: slots x n work elements
@@ -121,6 +124,9 @@ struct mm_b200_batch {
     std::vector<uint32_t> nbits, pos;
     bool exp_dirty = false;
     uint64_t launches = 0;
+    uint2* d_items = nullptr;          // run_items: the list on the device and its pinned staging
+    uint2* h_items = nullptr;
+    cudaEvent_t items_copied = nullptr;   // the staging may be rewritten once this has passed
 };
 
 namespace {
@@ -151,7 +157,7 @@ int ensure_tables(mm_b200_device* dev, int m, bool global, const DevTables** out
                                    cudaSharedmemCarveoutMaxShared));
         dev->global_configured = true;
     }
-    if (!global && !dev->configured[m]) {
+    if (!global && m <= kMaxSharedLogN && !dev->configured[m]) {
         KernelSet ks;
         kernel_set(m, ks);
         MM_CK(cudaFuncSetAttribute((const void*)ks.step, cudaFuncAttributeMaxDynamicSharedMemorySize, ks.smem));
@@ -281,8 +287,17 @@ int launch_steps(mm_b200_batch* b, size_t bits, bool bare = false) {
     const size_t chunk = (size_t)std::max(1, b->sched.launch_steps > 0 ? b->sched.launch_steps : b->dev->max_launch_steps);
     while (left > 0) {
         const uint32_t s = (uint32_t)std::min(left, chunk);
-        if (b->global) b->gk.step<<<(unsigned)b->slots, b->gk.threads, b->gk.smem, b->stream>>>(g, 0, s);
-        else b->ks.step<<<(unsigned)b->slots, b->ks.threads, b->ks.smem, b->stream>>>(a, 0, s);
+        if (b->cluster) {
+            SlotArgs c = a;
+            c.tab2 = b->ctab->t2;
+            c.tab1 = b->ctab->t1;
+            const int e = cluster_launch(b->m, c, (uint32_t)b->slots, s, b->stream);
+            if (e) return fail(MM_ERR_CUDA, std::string("cluster launch: ") + cudaGetErrorString((cudaError_t)e));
+        } else if (b->global) {
+            b->gk.step<<<(unsigned)b->slots, b->gk.threads, b->gk.smem, b->stream>>>(g, 0, s);
+        } else {
+            b->ks.step<<<(unsigned)b->slots, b->ks.threads, b->ks.smem, b->stream>>>(a, 0, s, nullptr);
+        }
         MM_CK(cudaGetLastError());
         ++b->launches;
         for (size_t i = 0; i < b->slots; ++i) b->pos[i] += std::min<uint32_t>(s, b->nbits[i] - b->pos[i]);
@@ -304,6 +319,24 @@ int ensure_global_buffers(mm_b200_batch* b) {
     if (!b->d_w2) {
         MM_CK(cudaMalloc(&b->d_w2, b->slots * b->n * sizeof(F2)));
         MM_CK(cudaMalloc(&b->d_w1, b->slots * b->n * sizeof(F1)));
+    }
+    return MM_OK;
+}
+
+// Cluster mode of a global batch: the shared-layout tables of its length and the kernels' shared
+// memory opt-in (once per device).
+int ensure_cluster(mm_b200_batch* b) {
+    if (!b->ctab) {
+        const DevTables* t = nullptr;
+        int rc = ensure_tables(b->dev, b->m, false, &t);
+        if (rc) return rc;
+        b->ctab = t;
+    }
+    std::lock_guard<std::mutex> lock(b->dev->mu);
+    if (!b->dev->cluster_configured) {
+        const int e = cluster_configure();
+        if (e) return fail(MM_ERR_CUDA, std::string("cluster mode: ") + cudaGetErrorString((cudaError_t)e));
+        b->dev->cluster_configured = true;
     }
     return MM_OK;
 }
@@ -682,6 +715,55 @@ int mm_b200_mul(mm_b200_batch* b, size_t out, size_t a, size_t bb) {
     return check_err(b, "mul");
 }
 
+int mm_b200_run_items_async(mm_b200_batch* b, size_t count, const size_t* slots, const uint32_t* steps) {
+    if (!b || (count && (!slots || !steps))) return fail(MM_ERR_ARG, "run_items: null argument");
+    if (b->global || b->cluster) return fail(MM_ERR_UNSUPPORTED, "run_items: shared-memory lengths only (L <= 16384)");
+    if (count == 0) return MM_OK;
+    int rc = check_slot_list(b, count, slots, "run_items");
+    if (rc) return rc;
+    std::vector<char> seen(b->slots, 0);
+    for (size_t i = 0; i < count; ++i) {
+        if (seen[slots[i]]) return fail(MM_ERR_ARG, "run_items: slot listed twice");
+        if (steps[i] == 0) return fail(MM_ERR_ARG, "run_items: a step budget must be at least 1");
+        seen[slots[i]] = 1;
+    }
+    MM_CK(cudaSetDevice(b->dev->device));
+    rc = push(b);
+    if (rc) return rc;
+    if (!b->d_items) {
+        MM_CK(cudaMalloc(&b->d_items, b->slots * sizeof(uint2)));
+        MM_CK(cudaMallocHost(&b->h_items, b->slots * sizeof(uint2)));
+        MM_CK(cudaEventCreateWithFlags(&b->items_copied, cudaEventDisableTiming));
+    } else {
+        MM_CK(cudaEventSynchronize(b->items_copied));   // the previous list has left the staging
+    }
+    for (size_t i = 0; i < count; ++i) b->h_items[i] = make_uint2((unsigned)slots[i], steps[i]);
+    MM_CK(cudaMemcpyAsync(b->d_items, b->h_items, count * sizeof(uint2), cudaMemcpyHostToDevice, b->stream));
+    MM_CK(cudaEventRecord(b->items_copied, b->stream));
+    SlotArgs a = slot_args(b);
+    for (size_t first = 0; first < count; first += 65535) {
+        const unsigned grid = (unsigned)std::min<size_t>(65535, count - first);
+        b->ks.step<<<grid, b->ks.threads, b->ks.smem, b->stream>>>(a, 0, 0, b->d_items + first);
+        MM_CK(cudaGetLastError());
+        ++b->launches;
+    }
+    for (size_t i = 0; i < count; ++i) {
+        const size_t s = slots[i];
+        b->pos[s] += std::min<uint32_t>(steps[i], b->nbits[s] - b->pos[s]);
+    }
+    b->host_x_valid = false;
+    return MM_OK;
+}
+
+int mm_b200_blocks_per_sm(const mm_b200_batch* b) {
+    if (!b) return 0;
+    int per = 0;
+    if (b->cluster || b->global) return b->cluster ? 1 : 2;
+    if (cudaSetDevice(b->dev->device) != cudaSuccess) return 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, b->ks.step, b->ks.threads, b->ks.smem) != cudaSuccess) return 0;
+    return per;
+}
+
 int mm_b200_wait_check(mm_b200_batch* b, uint64_t limit_ns) {
     if (!b) return fail(MM_ERR_ARG, "null batch");
     if (limit_ns < 1000 || limit_ns > 1000000000ull) return fail(MM_ERR_ARG, "wait_check: limit must be 1 us .. 1 s");
@@ -738,22 +820,35 @@ void mm_b200_destroy(mm_b200_batch* b) {
     if (b->stream) cudaStreamDestroy(b->stream);
     if (b->host_x) cudaFreeHost(b->host_x);
     if (b->host_exp) cudaFreeHost(b->host_exp);
+    if (b->d_items) cudaFree(b->d_items);
+    if (b->h_items) cudaFreeHost(b->h_items);
+    if (b->items_copied) cudaEventDestroy(b->items_copied);
     delete b;
 }
 
 int mm_b200_set_schedule(mm_b200_batch* b, const mm_b200_schedule* sc) {
     if (!b || !sc) return fail(MM_ERR_ARG, "set_schedule: null argument");
     if (sc->launch_steps < 0 || sc->step_ns < 0) return fail(MM_ERR_ARG, "set_schedule: negative value");
+    if (sc->global < 0 || sc->global > 2) return fail(MM_ERR_ARG, "set_schedule: mode must be 0, 1 or 2");
     MM_CK(cudaSetDevice(b->dev->device));
     const bool global = sc->global != 0;
+    const bool cluster = sc->global == 2;
     if (!global && b->m > kMaxSharedLogN) return fail(MM_ERR_UNSUPPORTED, "set_schedule: L > 16384 runs in global mode only");
+    if (cluster && (b->m < kMinClusterLogN || b->m > kMaxClusterLogN))
+        return fail(MM_ERR_UNSUPPORTED, "set_schedule: cluster mode runs L = 32768 and 65536 only");
+    if (cluster && b->plain) return fail(MM_ERR_UNSUPPORTED, "set_schedule: cluster mode needs the wraparound path");
     if (global) {
         int rc = ensure_global_buffers(b);
         if (rc) return rc;
     }
+    if (cluster) {
+        int rc = ensure_cluster(b);
+        if (rc) return rc;
+    }
     b->global = global;
+    b->cluster = cluster;
     b->sched = *sc;
-    b->sched.global = global ? 1 : 0;
+    b->sched.global = cluster ? 2 : (global ? 1 : 0);
     return MM_OK;
 }
 

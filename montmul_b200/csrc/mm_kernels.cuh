@@ -277,12 +277,20 @@ __device__ __forceinline__ void step_slot(const SlotArgs& a, uint32_t slot, uint
     }
 }
 
-// The uniform launch: one block per slot first + blockIdx.x.
+// The uniform launch: one block per slot first + blockIdx.x, `bits` steps each; or, with an item
+// list, one block per item (slot, steps) of the list (a serving tick's launch over the busy slots
+// of a batch; each slot at most once).
 template <int M, int NT>
-__global__ void __launch_bounds__(NT, (M <= 12 ? 2 : 1)) step_kernel(SlotArgs a, uint32_t first, uint32_t bits) {
+__global__ void __launch_bounds__(NT, (M <= 12 ? 2 : 1))
+    step_kernel(SlotArgs a, uint32_t first, uint32_t bits, const uint2* __restrict__ items) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ uint64_t sc[CarryScratch<NT>::words];
-    step_slot<M, NT>(a, first + blockIdx.x, bits, smem_raw, sc);
+    if (items) {
+        const uint2 it = items[blockIdx.x];
+        step_slot<M, NT>(a, it.x, it.y, smem_raw, sc);
+    } else {
+        step_slot<M, NT>(a, first + blockIdx.x, bits, smem_raw, sc);
+    }
 }
 
 // x[out] <- x[ia] x[ib] R^-1 with slot out's modulus (cpu.rs:558-571), one block. spec: n

@@ -35,6 +35,7 @@ def _lib():
             ("__gmpz_export", [vp, C.POINTER(C.c_size_t), C.c_int, C.c_size_t, C.c_int, C.c_size_t, P], vp),
             ("__gmpz_sizeinbase", [P, C.c_int], C.c_size_t),
             ("__gmpz_powm", [P, P, P, P], None),
+            ("__gmpz_gcd", [P, P, P], None),
             ("__gmpz_mul", [P, P, P], None),
             ("__gmpz_mod", [P, P, P], None),
             ("__gmpz_invert", [P, P, P], C.c_int),
@@ -105,6 +106,13 @@ def mulmod(a: int, b: int, m: int) -> int:
     r, aa, bb, mm = Mpz(), Mpz(a), Mpz(b), Mpz(m)
     _f("mpz_mul")(C.byref(r.z), C.byref(aa.z), C.byref(bb.z))
     _f("mpz_mod")(C.byref(r.z), C.byref(r.z), C.byref(mm.z))
+    return r.get()
+
+
+def gcd(a: int, b: int) -> int:
+    """gcd(a, b) of nonnegative integers (GMP's subquadratic gcd; Python's is quadratic)."""
+    r, aa, bb = Mpz(), Mpz(a), Mpz(b)
+    _f("mpz_gcd")(C.byref(r.z), C.byref(aa.z), C.byref(bb.z))
     return r.get()
 
 

@@ -21,7 +21,9 @@ verdict runs from its arrival to the tick that read its result.
 """
 from __future__ import annotations
 
+import json
 import math
+import os
 import statistics
 import time
 from collections import deque
@@ -33,9 +35,15 @@ from . import gmp
 from .batch import ModBatch, MontMulError, Params
 
 MAX_DRAW = 1 << 30
-# Exponents p of Mersenne primes 2^p - 1 (Lucas-Lehmer; the published list), used as the prime
-# requests of the stream: a seeded next_prime search at these sizes takes far longer than the run.
+# Prime requests up to this size are seeded next_prime primes; above it a seeded next_prime search
+# takes far longer than the run (minutes per prime at 16,000 bits, hours at 200,000), so a Mersenne
+# prime 2^p - 1 of about the drawn size stands in.
+PRIME_LIMIT_BITS = 16_000
+# Exponents p of Mersenne primes 2^p - 1 (Lucas-Lehmer; the published list).
 MERSENNE_P = (4253, 4423, 9689, 9941, 11213, 19937, 21701, 23209, 44497, 86243, 110503, 132049, 216091)
+# next_prime(start) - start of the prime requests of the default stream, written by
+# data/make_serve_primes.py (GMP's mpz_nextprime); other streams search at run time.
+PRIMES_FIXTURE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "serve_primes.json")
 
 
 @dataclass
@@ -46,7 +54,7 @@ class Request:
     arrival: float        # seconds after the start of the run
     a: int = 0
     b: int = 0
-    prime: bool = False   # drawn as a known prime
+    prime: str = ""       # "next_prime" or "mersenne" for a request drawn as a known prime
     length: int = 0
     admitted: Optional[float] = None
     done: Optional[float] = None
@@ -55,13 +63,38 @@ class Request:
     raw: Optional[int] = None
 
 
+def fixture_offsets(seed: int, lo: int, hi: int, prime_frac: float, mul_frac: float,
+                    prime_limit: int = PRIME_LIMIT_BITS) -> dict:
+    """{rid: next_prime(start) - start} for the stream these parameters draw, if the fixture
+    covers it; else {}."""
+    try:
+        with open(PRIMES_FIXTURE) as f:
+            fx = json.load(f)
+    except OSError:
+        return {}
+    if (fx["seed"], fx["lo"], fx["hi"], fx["prime_frac"], fx["mul_frac"], fx["limit_bits"]) != \
+            (seed, lo, hi, prime_frac, mul_frac, prime_limit):
+        return {}
+    return {int(k): int(v) for k, v in fx["offsets"].items()}
+
+
+def mersenne_near(bits: int, lo: int, hi: int) -> int:
+    """The Mersenne exponent in [lo, hi] nearest to `bits` on a log scale."""
+    cands = [p for p in MERSENNE_P if lo <= p <= hi] or list(MERSENNE_P)
+    return min(cands, key=lambda p: abs(math.log(p / bits)))
+
+
 def stream(count: int, rate: float, lo: int, hi: int, prime_frac: float = 0.1, mul_frac: float = 0.05,
-           seed: int = 2026):
-    """`count` requests with exponential inter-arrival times of mean 1/rate: bit sizes log-uniform
-    in [lo, hi]; a `prime_frac` share are Mersenne primes in range, a `mul_frac` share mul
-    requests, the rest random odd N with the top bit set (composite but for a vanishing share)."""
+           seed: int = 2026, prime_source=None, prime_limit: int = PRIME_LIMIT_BITS):
+    """`count` requests with exponential inter-arrival times of mean 1/rate and bit sizes
+    log-uniform in [lo, hi], all drawn from GMP's generator seeded `seed`: a `mul_frac` share are
+    mul requests (random a, b below a random odd N), a `prime_frac` share are primes, the rest
+    random odd N with the top bit set (composite but for a vanishing share). A prime request draws
+    a random start of its size with the top bit set; up to `prime_limit` bits its N is
+    next_prime(start) (from the fixture, else `prime_source(rid, bits, start)`, else computed),
+    above it the Mersenne prime nearest its size stands in."""
     rng = gmp.RandState(seed)
-    primes = [p for p in MERSENNE_P if lo <= p <= hi]
+    offsets = fixture_offsets(seed, lo, hi, prime_frac, mul_frac, prime_limit)
     out, t = [], 0.0
     for rid in range(count):
         u = (rng.random_below(MAX_DRAW - 1) + 1) / MAX_DRAW
@@ -72,9 +105,18 @@ def stream(count: int, rate: float, lo: int, hi: int, prime_frac: float = 0.1, m
         if kind_draw < mul_frac:
             n = rng.random_bits(bits) | (1 << (bits - 1)) | 1
             out.append(Request(rid, "mul", n, t, a=rng.random_below(n), b=rng.random_below(n)))
-        elif kind_draw < mul_frac + prime_frac and primes:
-            p = primes[rng.random_below(len(primes))]
-            out.append(Request(rid, "fermat", (1 << p) - 1, t, prime=True))
+        elif kind_draw < mul_frac + prime_frac:
+            start = rng.random_bits(bits) | (1 << (bits - 1))
+            if bits > prime_limit:
+                out.append(Request(rid, "fermat", (1 << mersenne_near(bits, lo, hi)) - 1, t, prime="mersenne"))
+                continue
+            if rid in offsets:
+                p = start + offsets[rid]
+            elif prime_source is not None:
+                p = prime_source(rid, bits, start)
+            else:
+                p = gmp.next_prime(start)
+            out.append(Request(rid, "fermat", p, t, prime="next_prime"))
         else:
             n = rng.random_bits(bits) | (1 << (bits - 1)) | 1
             out.append(Request(rid, "fermat", n, t))
@@ -96,7 +138,7 @@ class Server:
     """Lanes of segments per transform length, one plan over every segment."""
 
     def __init__(self, dev, base: int = 3, quantum: int = 128, segment_slots: int = 0, budget_frac: float = 0.5,
-                 tuned: bool = True):
+                 tuned: bool = True, checker: Optional["VerdictChecker"] = None):
         from .backend import lib
         self.dev = dev
         self.lib = lib()
@@ -112,10 +154,12 @@ class Server:
         self.tuned = tuned
         self.steps_done = 0
         self.gpu_s = 0.0          # wall time inside plan launches (launch, run, wait)
+        self.host_s = {"admit": 0.0, "list": 0.0, "read": 0.0}   # host time between launches
         self.ticks = []           # (t, busy slots, slot-steps run)
         from . import tune
         self.table = tune.load_table().get(dev.device_name(), {})
         self.seg_steps = []       # per plan batch: steps of one tick
+        self.checker = checker    # receives every finished Fermat request
 
     # ---- admission ----
     def _grow(self, length: int) -> Optional[Segment]:
@@ -255,13 +299,16 @@ class Server:
 
     def tick(self) -> int:
         """One quantum on every busy slot, then the finished slots are read and freed."""
+        t = time.perf_counter()
         plan = self._plan()
         items = self.work_list()
         run = sum(it[2] for it in items)
-        t = time.perf_counter()
+        t1 = time.perf_counter()
+        self.host_s["list"] += t1 - t
         plan.run_items([it[0] for it in items], [it[1] for it in items], [it[2] for it in items])
-        self.gpu_s += time.perf_counter() - t
-        now = time.perf_counter() - self.t0
+        t2 = time.perf_counter()
+        self.gpu_s += t2 - t1
+        now = t2 - self.t0
         self.steps_done += run
         self.ticks.append((now, self.busy(), run))
         finished = 0
@@ -277,8 +324,11 @@ class Server:
                     r.raw = raw
                     r.verdict = raw == m.r or raw == m.r + m.n
                     r.done = now
+                    if self.checker is not None:
+                        self.checker.submit(r)
                     seg.free.append(s)
                     finished += 1
+        self.host_s["read"] += time.perf_counter() - t2
         return finished
 
     def serve(self, reqs):
@@ -292,7 +342,9 @@ class Server:
             while pending and pending[0].arrival <= now:
                 waiting.append(pending.popleft())
             if waiting:
+                t = time.perf_counter()
                 self.admit(waiting, now)
+                self.host_s["admit"] += time.perf_counter() - t
             if self.busy():
                 self.completed += self.tick()
             elif pending and not waiting:
@@ -318,13 +370,86 @@ def capacity(reqs, step_s) -> float:
 _LENGTHS = [1 << e for e in range(3, 25)]
 
 
-def check(dev, reqs, gmp_bits: int = 20_000, sample: int = 24, seed: int = 2027, threads: int = 32) -> dict:
-    """Checks the served results: every mul against a b mod N; every Fermat verdict of at most
-    `gmp_bits` bits against GMP's pow_mod(3, N - 1, N) == 1 (GMP takes minutes per test at 200,000
-    bits); every known prime must be a PRP; and `sample` seeded larger requests are run again
-    alone, one uniform batch per length, and must end with the same raw Montgomery limbs (the
-    uniform batches are the path the test suite pins to the reference Cpu backend)."""
-    out = {"mul": 0, "gmp": 0, "primes": 0, "alone": 0}
+def odd_primes_below(bound: int):
+    """The odd primes below `bound` (sieve of Eratosthenes over odd numbers)."""
+    s = bytearray([1]) * (bound // 2)   # s[i] stands for 2 i + 1
+    s[0] = 0
+    i = 1
+    while (2 * i + 1) ** 2 < bound:
+        if s[i]:
+            p = 2 * i + 1
+            s[p * p // 2::p] = bytes(len(range(p * p // 2, bound // 2, p)))
+        i += 1
+    return [2 * i + 1 for i in range(bound // 2) if s[i]]
+
+
+def product(v):
+    while len(v) > 1:
+        v = [v[i] * v[i + 1] if i + 1 < len(v) else v[i] for i in range(0, len(v), 2)]
+    return v[0]
+
+
+class VerdictChecker:
+    """Decides, for every served Fermat request, the verdict rug's pow_mod(3, N - 1, N) == 1 gives,
+    in a host thread pool while the stream runs, and requires the served verdict to equal it.
+    Each decision is exact, by the cheapest of three routes:
+
+      - N a Mersenne prime 2^p - 1 (proven prime): 3^(N-1) = 1 mod N by Fermat's little theorem;
+      - N with a factor below SMALL_PRIME_BOUND: g = gcd(N, product of those primes) > 1, and if
+        3^(N-1) mod g != 1 then 3^(N-1) mod N != 1 (g divides N), so the verdict is false;
+      - otherwise (no small factor, the next_prime primes, or 3^(N-1) = 1 mod g): GMP's mpz_powm
+        itself, the call rug's pow_mod makes.
+
+    GMP releases the interpreter lock inside each call, so the pool runs beside the serving loop."""
+
+    SMALL_PRIME_BOUND = 1 << 20
+
+    def __init__(self, threads: int = 0):
+        self.threads = threads or max(1, (os.cpu_count() or 2) - 2)
+        self.small = product(odd_primes_below(self.SMALL_PRIME_BOUND))
+        self.ex = ThreadPoolExecutor(self.threads)
+        self.futs = []
+
+    def submit(self, r: Request) -> None:
+        if r.kind == "fermat":
+            self.futs.append(self.ex.submit(self._one, r))
+
+    def _one(self, r: Request) -> str:
+        if r.prime == "mersenne":
+            want, how = True, "mersenne_prime"
+        else:
+            want, how = None, "gmp_powm"
+            g = gmp.gcd(r.n, self.small)
+            if g > 1 and gmp.powm(3, r.n - 1, g) != 1:
+                want, how = False, "small_factor"
+            if want is None:
+                want = gmp.powm(3, r.n - 1, r.n) == 1
+        if r.verdict != want:
+            raise MontMulError(f"request {r.rid} ({r.n.bit_length()} bits): verdict {r.verdict} disagrees with "
+                               f"pow_mod ({want}, by {how})")
+        return how
+
+    def finish(self) -> dict:
+        out = {"mersenne_prime": 0, "small_factor": 0, "gmp_powm": 0}
+        try:
+            for f in self.futs:
+                out[f.result()] += 1
+        finally:
+            self.ex.shutdown(wait=True, cancel_futures=True)
+        out["verdicts"] = sum(out.values())
+        return out
+
+
+def check(dev, reqs, checked: dict, sample: int = 24, seed: int = 2027) -> dict:
+    """The served results beyond the verdicts (`checked`, from VerdictChecker): every mul against
+    a b mod N, every drawn prime a PRP, and `sample` seeded requests run again alone, one uniform
+    batch per length, ending with the same raw Montgomery limbs as in the mix (the uniform batches
+    are the path the test suite pins to the reference Cpu backend)."""
+    out = dict(checked)
+    out.update({"mul": 0, "primes": 0, "alone": 0})
+    ferm = [r for r in reqs if r.kind == "fermat"]
+    if out["verdicts"] != len(ferm):
+        raise MontMulError(f"{out['verdicts']} verdicts checked of {len(ferm)} Fermat requests")
     for r in reqs:
         if r.kind == "mul":
             if r.value != r.a * r.b % r.n:
@@ -332,22 +457,13 @@ def check(dev, reqs, gmp_bits: int = 20_000, sample: int = 24, seed: int = 2027,
             out["mul"] += 1
         elif r.prime:
             if not r.verdict:
-                raise MontMulError(f"request {r.rid}: the prime 2^{r.n.bit_length()} - 1 was not a PRP")
+                raise MontMulError(f"request {r.rid}: the prime of {r.n.bit_length()} bits was not a PRP")
             out["primes"] += 1
-    small = [r for r in reqs if r.kind == "fermat" and r.n.bit_length() <= gmp_bits]
-
-    def one(r):
-        if r.verdict != (gmp.powm(3, r.n - 1, r.n) == 1):
-            raise MontMulError(f"request {r.rid} ({r.n.bit_length()} bits): verdict disagrees with pow_mod")
-        return 1
-
-    with ThreadPoolExecutor(threads) as ex:
-        out["gmp"] = sum(ex.map(one, small))
-    big = [r for r in reqs if r.kind == "fermat" and r.n.bit_length() > gmp_bits]
     rng = gmp.RandState(seed)
+    pool = list(ferm)
     picked = []
-    while big and len(picked) < sample:
-        picked.append(big.pop(rng.random_below(len(big))))
+    while pool and len(picked) < sample:
+        picked.append(pool.pop(rng.random_below(len(pool))))
     by_len = {}
     for r in picked:
         by_len.setdefault(r.length, []).append(r)
@@ -387,7 +503,8 @@ def summarize(server: Server, reqs, uniform_modsq: float, rate: float, cap: floa
     return {
         "offered_tests_per_s": rate, "capacity_tests_per_s": cap, "load": rate / cap,
         "requests": len(reqs), "fermat": len(ferm), "mul": len(muls),
-        "primes": sum(1 for r in ferm if r.prime), "prp": sum(1 for r in ferm if r.verdict),
+        "primes": sum(1 for r in ferm if r.prime), "next_prime_primes": sum(1 for r in ferm if r.prime == "next_prime"),
+        "mersenne_primes": sum(1 for r in ferm if r.prime == "mersenne"), "prp": sum(1 for r in ferm if r.verdict),
         "seconds": end, "tests_per_hour": 3600.0 * len(ferm) / end,
         "modsq_per_s": steps / end, "steady_modsq_per_s": win_modsq,
         "uniform_modsq_per_s": uniform_modsq,
@@ -397,6 +514,7 @@ def summarize(server: Server, reqs, uniform_modsq: float, rate: float, cap: floa
         "ticks": len(server.ticks), "quantum": server.quantum,
         "busy_slots_p50": percentile([b for t, b, _ in server.ticks if t_a <= t <= t_b], 0.5),
         "launch_time_frac": server.gpu_s / end,
+        "host_time_frac": {k: v / end for k, v in server.host_s.items()},
         "lanes": {str(L): sum(len(s.batch.moduli) for s in segs) for L, segs in server.lanes.items()},
         "device_bytes": server.used,
     }
@@ -404,6 +522,7 @@ def summarize(server: Server, reqs, uniform_modsq: float, rate: float, cap: floa
 
 def main(args) -> dict:
     from .backend import B200
+    from .clocks import ClockSampler
     from . import tune
     dev = B200(device=args.device)
     lengths = dev.supported_lengths()
@@ -426,12 +545,16 @@ def main(args) -> dict:
         rate = load * cap
         count = max(8, int(round(rate * args.duration)))
         reqs = stream(count, rate, args.lo, args.hi, seed=args.seed)
-        srv = Server(dev, quantum=args.quantum)
-        srv.serve(reqs)
+        checker = None if args.no_check else VerdictChecker()
+        srv = Server(dev, quantum=args.quantum, checker=checker)
+        with ClockSampler(args.device) as clk:
+            srv.serve(reqs)
         srv.close()
         s = summarize(srv, reqs, uniform, rate, cap)
-        s["checked"] = check(dev, reqs) if not args.no_check else None
+        s["clocks"] = clk.summary()
+        s["checked"] = check(dev, reqs, checker.finish()) if checker is not None else None
         results.append(s)
     return {"workload": f"Poisson arrivals for {args.duration} s, bits log-uniform in [{args.lo}, {args.hi}], "
-                        f"10% Mersenne primes, 5% mul, full base-3 Fermat tests (seed {args.seed})",
+                        f"10% primes (seeded next_prime up to {PRIME_LIMIT_BITS} bits, Mersenne primes of about the "
+                        f"drawn size above), 5% mul, full base-3 Fermat tests (seed {args.seed})",
             "loads": results}

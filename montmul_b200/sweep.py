@@ -69,7 +69,7 @@ def one_size(dev, bits: int, slots: int, ebits: int, seed: int = 2026) -> dict:
     rate = slots * e_bits / secs
     return {"bits": bits, "L": length, "slots": slots, "ebits": e_bits, "seconds": secs, "modsq_per_s": rate,
             "bitsteps_per_s": rate * bits, "gbfly_per_s": rate * butterfly_pairs(n) / 1e9,
-            "mode": "global" if sched["global"] else "shared", "tuned": tuned, "mul_checked": muls,
+            "mode": sched["mode"], "tuned": tuned, "mul_checked": muls,
             "clocks": clk.summary()}
 
 

@@ -4,8 +4,11 @@ fixes the schedule: montmul/src/gpu/plan.rs:26-60).
 For each transform length L the tuner times every schedule the library can switch at run time on
 the device and keeps the fastest:
 
-  - shared vs global mode: L <= 4096 shared only, L = 8192 and 16384 both (16384 in shared mode
-    holds one block per SM, in global mode two), L >= 32768 global only;
+  - the mode: shared memory, global mode or cluster mode. L <= 4096 run in shared memory only;
+    L = 8192 and 16384 in shared memory or global mode (16384 in shared memory holds one block per
+    SM, in global mode two); L = 32768 and 65536 in global mode or cluster mode (a thread-block
+    cluster of L / 16384 blocks per slot with the vector in the cluster's shared memory); longer
+    lengths in global mode only;
   - steps per launch (launch_steps): a longer launch saves launch gaps, a shorter one bounds how
     long a batch holds the GPU.
 
@@ -64,9 +67,21 @@ def threads_for(m: int) -> int:
     return 32 if m - 3 <= 5 else (256 if m - 3 >= 8 else 1 << (m - 3))
 
 
-def fixed_parts(length: int, global_mode: bool):
+SHARED, GLOBAL, CLUSTER = 0, 1, 2
+MIN_CLUSTER_N, MAX_CLUSTER_N = 16384, 32768   # L = 32768 and 65536
+CLUSTER_CHUNK = 8192                          # elements per block of a cluster
+
+
+def mode_name(mode) -> str:
+    return ("shared", "global", "cluster")[int(mode)]
+
+
+def fixed_parts(length: int, global_mode):
     n = length // 2
     m = n.bit_length() - 1
+    if int(global_mode) == CLUSTER:
+        return {"threads": 512, "blocks_per_sm": 1, "cluster": n // CLUSTER_CHUNK, "tile": None,
+                "radix": radix_schedule(m)}
     if global_mode:
         g = m - TILE.bit_length() + 1
         return {"threads": 256, "blocks_per_sm": 2, "tile": TILE,
@@ -79,9 +94,11 @@ def candidates(length: int):
     n = length // 2
     modes = []
     if n <= MAX_SHARED_N:
-        modes.append(False)
+        modes.append(SHARED)
     if n >= MIN_GLOBAL_N:
-        modes.append(True)
+        modes.append(GLOBAL)
+    if MIN_CLUSTER_N <= n <= MAX_CLUSTER_N:
+        modes.append(CLUSTER)
     return [(g, s) for g in modes for s in LAUNCH_STEPS]
 
 
@@ -148,8 +165,11 @@ def tune_length(dev, length: int, budget_s: float = 4.0):
     for g, s in cands:
         sec = measure(dev, length, g, s, slots, steps)
         results.append({"global": g, "launch_steps": s, "step_ns": sec * 1e9})
-    best = min(results, key=lambda r: r["step_ns"])
+    ranked = sorted(results, key=lambda r: r["step_ns"])
+    best = ranked[0]
     out = dict(best)
+    if len(ranked) > 1:
+        out["runner_up"] = dict(ranked[1])
     out.update(fixed_parts(length, best["global"]))
     out["slots"] = slots
     out["steps"] = steps
@@ -215,7 +235,7 @@ def tune(dev, lengths, force: bool = False, log=print, mixed_only: bool = False)
             continue
         r = tune_length(dev, length)
         per[str(length)] = r
-        log(f"L={length}: {'global' if r['global'] else 'shared'} launch_steps={r['launch_steps']} "
+        log(f"L={length}: {mode_name(r['global'])} launch_steps={r['launch_steps']} "
             f"{r['step_ns'] / 1e3:.2f} us/slot-step")
         save_table(table)
     return per

@@ -122,3 +122,60 @@ def test_bounded_wait_runs_out_and_context_stays_usable(gpu, wrap, bits):
     assert [b.read_raw(i) for i in range(3)] == [ref.read_raw(i) for i in range(3)]
     for i, (n, e) in enumerate(zip(moduli, exps)):
         assert b.read(i) == powm(5 + i, 1 << e.bit_length(), n) * powm(3, e, n) % n
+
+
+@pytest.mark.parametrize("length,steps", [(1 << 15, 10), (1 << 16, 6)])
+def test_cluster_mode_same_raw_as_oracle(gpu, wrap, length, steps):
+    """Cluster mode (one thread-block cluster of L / 16384 blocks per slot, the vector in the
+    cluster's shared memory) at the top of the bucket: raw limbs equal Cpu::with_wraparound."""
+    dev = gpu()
+
+    class Cluster:
+        def __getattr__(self, name):
+            return getattr(dev, name)
+
+        def create(self, *a):
+            st = dev.create(*a)
+            dev.set_schedule(st, 2, 0)
+            assert dev.get_schedule(st)["mode"] == "cluster"
+            return st
+
+    common.same_raw(lambda: Cluster(), wrap, 16 * length - 4, 3, steps)
+
+
+@pytest.mark.parametrize("bits", [300_000, 1_000_000])
+def test_cluster_mode_equals_global_mode_and_pow_mod(gpu, bits):
+    """The same batch stepped in cluster mode, then switched to global mode and on, ends with the
+    raw limbs of a global-mode run and the value pow_mod gives; a bare step leaves x alone."""
+    rng = RandState(bits + 11)
+    moduli = [common.rand_odd(rng, bits) for _ in range(5)]
+    exps = [common.rand_exponent(rng, 30) for _ in range(5)]
+    runs = []
+    for modes in ((1, 1), (2, 1), (2, 2)):
+        b = ModBatch(gpu(), moduli, 3)
+        be, st = b.backend_and_state()
+        b.load_all([2, 3, 4, 5, 6])
+        b.set_exponents(exps)
+        be.set_schedule(st, modes[0], 7)
+        b.run(13)
+        be.set_schedule(st, modes[1], 7)
+        b.run(30)
+        runs.append([b.read_raw(i) for i in range(5)])
+        for i, (n, e) in enumerate(zip(moduli, exps)):
+            assert b.read(i) == powm(2 + i, 1 << e.bit_length(), n) * powm(3, e, n) % n
+    assert runs[0] == runs[1] == runs[2]
+    b = ModBatch(gpu(), moduli[:2], 3)
+    be, st = b.backend_and_state()
+    be.set_schedule(st, 2, 0)
+    b.load_all([7, 8])
+    b.set_exponents(exps[:2])
+    before = [b.read_raw(i) for i in range(2)]
+    be.run_bare(st, 5)
+    assert [b.read_raw(i) for i in range(2)] == before and b.remaining(0) == exps[0].bit_length() - 5
+
+
+def test_cluster_mode_rejects_other_lengths(gpu):
+    b = ModBatch(gpu(), [common.rand_odd(RandState(3), 100_000)], 3)
+    be, st = b.backend_and_state()
+    with pytest.raises(MontMulError, match="cluster mode runs L = 32768 and 65536 only"):
+        be.set_schedule(st, 2, 0)

@@ -26,9 +26,13 @@ def _alone_raw(dev, n):
 
 def test_served_stream_same_as_alone(dev):
     from montmul_b200 import serve
-    reqs = serve.stream(40, 400.0, 2000, 40_000, prime_frac=0.2, mul_frac=0.1, seed=17)
-    # Small segments force several segments per lane and waiting requests.
-    srv = serve.Server(dev, quantum=64, segment_slots=6, tuned=False)
+    # Seeded next_prime primes up to 6,000 bits (a quick search), Mersenne primes above.
+    reqs = serve.stream(40, 400.0, 2000, 40_000, prime_frac=0.2, mul_frac=0.1, seed=20, prime_limit=6000)
+    assert {r.prime for r in reqs if r.prime} == {"next_prime", "mersenne"}
+    # Small segments force several segments per lane and waiting requests; every verdict is
+    # checked while the stream runs.
+    checker = serve.VerdictChecker(threads=4)
+    srv = serve.Server(dev, quantum=64, segment_slots=6, tuned=False, checker=checker)
     srv.serve(reqs)
     srv.close()
     assert all(r.done is not None for r in reqs)
@@ -42,12 +46,13 @@ def test_served_stream_same_as_alone(dev):
         if r.prime:
             assert r.verdict
         assert r.raw == _alone_raw(dev, r.n), f"request {r.rid} ({r.n.bit_length()} bits)"
-    c = serve.check(dev, reqs, gmp_bits=20_000, sample=5)
+    c = serve.check(dev, reqs, checker.finish(), sample=5)
     ferm = [r for r in reqs if r.kind == "fermat"]
     assert c["mul"] == len(reqs) - len(ferm)
     assert c["primes"] == sum(1 for r in ferm if r.prime)
-    assert c["gmp"] == sum(1 for r in ferm if r.n.bit_length() <= 20_000)
-    assert c["alone"] == min(5, sum(1 for r in ferm if r.n.bit_length() > 20_000))
+    assert c["verdicts"] == len(ferm) == c["mersenne_prime"] + c["small_factor"] + c["gmp_powm"]
+    assert c["mersenne_prime"] == sum(1 for r in ferm if r.prime == "mersenne")
+    assert c["alone"] == 5
 
 
 def test_fermat_driver_on_mersenne_primes(dev):

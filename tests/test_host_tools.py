@@ -6,7 +6,8 @@ import pytest
 
 from montmul_b200 import mixed, serve, tune
 from montmul_b200.__main__ import tribonacci
-from montmul_b200.batch import Params
+from montmul_b200.batch import MontMulError, Params
+from montmul_b200.gmp import powm
 
 LENGTHS = [1 << e for e in range(3, 25)]
 
@@ -21,11 +22,16 @@ def test_radix_schedule_covers_every_stage():
 
 
 def test_tune_candidates_by_length():
-    assert tune.candidates(4096) == [(False, s) for s in tune.LAUNCH_STEPS]
-    assert {g for g, _ in tune.candidates(8192)} == {False, True}
-    assert {g for g, _ in tune.candidates(16384)} == {False, True}
-    assert {g for g, _ in tune.candidates(32768)} == {True}
+    S, G, C = tune.SHARED, tune.GLOBAL, tune.CLUSTER
+    assert tune.candidates(4096) == [(S, s) for s in tune.LAUNCH_STEPS]
+    assert {g for g, _ in tune.candidates(8192)} == {S, G}
+    assert {g for g, _ in tune.candidates(16384)} == {S, G}
+    assert {g for g, _ in tune.candidates(32768)} == {G, C}
+    assert {g for g, _ in tune.candidates(65536)} == {G, C}
+    assert {g for g, _ in tune.candidates(131072)} == {G}
     assert tune.fixed_parts(1 << 20, True)["radix"]["global"] == tune.radix_schedule(19 - 11)
+    assert tune.fixed_parts(32768, C)["cluster"] == 2 and tune.fixed_parts(65536, C)["cluster"] == 4
+    assert [tune.mode_name(m) for m in (S, G, C, False, True)] == ["shared", "global", "cluster", "shared", "global"]
 
 
 def test_tune_table_roundtrip(tmp_path, monkeypatch):
@@ -84,8 +90,14 @@ def test_mixed_workload():
 
 
 def test_serve_stream():
-    r = serve.stream(400, 10.0, 10_000, 200_000, seed=3)
-    assert r == serve.stream(400, 10.0, 10_000, 200_000, seed=3)
+    seen = {}
+
+    def src(rid, bits, start):
+        seen[rid] = (bits, start)
+        return start | 1
+
+    r = serve.stream(400, 10.0, 10_000, 200_000, seed=3, prime_source=src)
+    assert r == serve.stream(400, 10.0, 10_000, 200_000, seed=3, prime_source=lambda rid, bits, start: start | 1)
     assert all(b.arrival > a.arrival for a, b in zip(r, r[1:]))
     gaps = [b.arrival - a.arrival for a, b in zip(r, r[1:])]
     assert 0.07 < sum(gaps) / len(gaps) < 0.13   # mean 1 / rate
@@ -93,12 +105,61 @@ def test_serve_stream():
     assert 5 <= kinds.count("mul") <= 40
     primes = [x for x in r if x.prime]
     assert 20 <= len(primes) <= 70
+    assert {x.prime for x in primes} == {"next_prime", "mersenne"}
     for x in primes:
-        assert x.n + 1 == 1 << x.n.bit_length() and x.n.bit_length() in serve.MERSENNE_P
+        if x.prime == "mersenne":
+            assert x.rid not in seen
+            assert x.n + 1 == 1 << x.n.bit_length() and x.n.bit_length() in serve.MERSENNE_P
+        else:
+            bits, start = seen[x.rid]
+            assert bits <= serve.PRIME_LIMIT_BITS and start.bit_length() == bits and x.n == start | 1
     for x in r:
         assert x.n % 2 == 1
         if x.kind == "mul":
             assert 0 <= x.a < x.n and 0 <= x.b < x.n
+
+
+def test_serve_primes_fixture_covers_the_default_stream():
+    """Every prime request of at most PRIME_LIMIT_BITS among the fixture's requests of the default
+    stream (seed 2026, [10,000, 200,000] bits) takes its prime from the fixture: a base-3 Fermat
+    probable prime just above the seeded start."""
+    import json
+    with open(serve.PRIMES_FIXTURE) as f:
+        fx = json.load(f)
+    assert (fx["seed"], fx["lo"], fx["hi"], fx["limit_bits"]) == (2026, 10_000, 200_000, serve.PRIME_LIMIT_BITS)
+    starts = {}
+
+    def fail(rid, bits, start):
+        raise AssertionError(f"request {rid} ({bits} bits) is not in the fixture")
+
+    r = serve.stream(fx["requests"], 1.0, 10_000, 200_000, seed=2026, prime_source=fail)
+    small = [x for x in r if x.prime == "next_prime"]
+    assert len(small) == len(fx["offsets"]) > 20
+    for x in small:
+        off = fx["offsets"][str(x.rid)]
+        assert 0 < off < 100_000 and x.n.bit_length() <= serve.PRIME_LIMIT_BITS
+        assert powm(3, x.n - 1, x.n) == 1
+
+
+def test_verdict_checker_routes_and_rejects():
+    """The served-verdict check decides pow_mod(3, N - 1, N) == 1 exactly: Mersenne primes by
+    Fermat's little theorem, composites with a small factor g by 3^(N-1) mod g, the rest with
+    GMP's powm; a served verdict that differs is an error."""
+    p, q = 1_000_000_007, 998_244_353          # primes above the small-prime bound
+    reqs = [serve.Request(0, "fermat", (1 << 4423) - 1, 0.0, prime="mersenne", verdict=True),
+            serve.Request(1, "fermat", 3 * ((1 << 5000) + 1) + 0, 0.0, verdict=False),
+            serve.Request(2, "fermat", 1_000_003 * ((1 << 3000) - 1), 0.0, verdict=False),
+            serve.Request(3, "fermat", p * q, 0.0, verdict=False),
+            serve.Request(4, "fermat", (1 << 521) - 1, 0.0, prime="next_prime", verdict=True),
+            serve.Request(5, "mul", 7, 0.0)]
+    c = serve.VerdictChecker(threads=2)
+    for r in reqs:
+        c.submit(r)
+    assert c.finish() == {"mersenne_prime": 1, "small_factor": 2, "gmp_powm": 2, "verdicts": 5}
+    bad = serve.VerdictChecker(threads=1)
+    bad.submit(serve.Request(9, "fermat", p * q, 0.0, verdict=True))
+    with pytest.raises(MontMulError, match="request 9"):
+        bad.finish()
 
 
 def test_capacity_and_percentile():
