@@ -41,7 +41,15 @@ def g_of_n(n: int) -> int:
 # dram__bytes_read.sum + dram__bytes_write.sum of one step_kernel launch of this workload, from
 # one ncu capture of `python -m montmul_b200.profile --slots SLOTS --steps STEPS --launches 2`
 # (second launch): the slots and steps per launch it ran, and its DRAM bytes.
-TRAFFIC_CAPTURE = {"slots": 1184, "steps_per_launch": 16, "dram_bytes": 360.3e6 + 95.6e6}
+TRAFFIC_CAPTURE = {"slots": 2368, "steps_per_launch": 64, "dram_bytes": 13403741696 + 8097713920}
+
+# The step kernel against the hardware, from one ncu capture of step_kernel<12, 512> on this
+# workload (296 slots x 16 steps, second launch): issue slots used, ALU pipe (integer add, logic,
+# shift, min: 2 cycles per warp instruction on a B200) and FMA-heavy pipe (IMAD, IMAD.WIDE)
+# cycles active. The integer pipes of a B200 SM (measured with single-instruction chains: 64
+# ALU-pipe and 64 IMAD lanes per clock) are the ceiling the butterfly peak below runs against.
+HW_CAPTURE = {"issue_active": 0.540, "alu_pipe": 0.556, "fmaheavy_pipe": 0.555, "warps_per_scheduler": 6.78,
+              "capture": "ncu of step_kernel<12, 512>, 296 slots x 16 steps"}
 
 # The uneven-size persistent batch: 2,000 slots, bits log-uniform in [8,192, 300,000] (seed 7),
 # c in {2, 3, 4}, the top 1,000 bits of N - 1; the plan replays its launch from a CUDA graph
@@ -389,6 +397,9 @@ def main(argv=None):
                 "note": "butterfly pairs (GF(p^2) product + add + sub in both fields), G(n)=%d per modsq at "
                         "L=8192; peak = the kernels' own arithmetic in register-resident chains on all SMs, "
                         "measured in this run" % g_of_n(n)}
+    roofline_hw = dict(HW_CAPTURE, note="fractions of the SM's issue slots and integer pipes the step kernel used "
+                                         "in an ncu capture; the butterfly roofline above counts the same arithmetic "
+                                         "against a register-resident chain of it")
     roofline_hbm = {"bound": "hbm", "achieved": achieved_gbs, "peak": hbm, "unit": "GB/s",
                     "frac": (achieved_gbs / hbm) if hbm else None,
                     "note": "48n B of per-slot constants per slot-step; peak of measured (MEASURED_PEAKS.json)"}
@@ -400,7 +411,7 @@ def main(argv=None):
                        "slots_per_gpu": slots, "bits": BITS, "ebits": EBITS, "L": 8192,
                        "parallelism": f"slots sharded over {world} GPU(s)", "l2": "flushed between steps"},
             "fermat_tests_per_hour": value * 3600.0 / BITS, "e2e": e2e, "roofline": roofline,
-            "roofline_hbm": roofline_hbm, "gpu_launches": launches, "clocks": clocks,
+            "roofline_hbm": roofline_hbm, "roofline_hw": roofline_hw, "gpu_launches": launches, "clocks": clocks,
             "checked": "slot 0, last and 2 seeded slots equal GMP pow_mod"}
     del batch, st
     if world == 1 and not args.no_mixed:

@@ -121,6 +121,10 @@ uint64_t mm_b200_launches(const mm_b200_batch *b);
  * batch's step kernel that one SM holds at once (0 on an error). */
 int mm_b200_run_items_async(mm_b200_batch *b, size_t count, const size_t *slots, const uint32_t *steps);
 int mm_b200_blocks_per_sm(const mm_b200_batch *b);
+/* 1 while work enqueued on the batch's stream is still running, 0 once it has finished (then
+ * mm_b200_sync returns at once with the error check): lets a loop service whichever batch is
+ * done while the others run. */
+int mm_b200_busy(const mm_b200_batch *b);
 
 /* Failure path of the bounded waits (no counterpart in the reference): every wait of a kernel on
  * a bulk copy gives up after a time limit (100 ms in the step kernels), sets the slot's error
@@ -174,16 +178,20 @@ size_t mm_b200_t_len(const mm_b200_tbuf *b);
 void mm_b200_t_free(mm_b200_tbuf *b);
 
 /* ---- Schedules (no counterpart in the reference, whose planner fixes them: gpu/plan.rs:26-60) ----
- * global: 1 runs the batch in global mode (L >= 8192), 0 with the whole vector in shared memory
- * (L <= 16384). Shared and global mode compute the same per-slot constants, so a batch may
- * switch at any time. launch_steps: steps per kernel launch of run (0: the device default).
- * step_ns: the measured time of one slot-step at full occupancy, which orders the items of a
- * mixed launch (0: a model of the transform work). The autotuner (montmul_b200.tune) measures
- * these per length and caches them. */
+ * global: the mode. 0 runs the batch with the whole vector in shared memory (L <= 16384), 1 in
+ * global mode (L >= 8192), 2 in cluster mode (L = 32768 and 65536: a thread-block cluster of
+ * L / 16384 blocks per slot with the vector in the cluster's shared memory). All modes compute
+ * the same per-slot constants, so a batch may switch at any time. launch_steps: steps per kernel
+ * launch of run (0: the device default). step_ns: the measured time of one slot-step at full
+ * occupancy, which orders the items of a mixed launch (0: a model of the transform work).
+ * threads: threads per block of the shared-memory step kernel (0: the length's default; L = 4096,
+ * 8192 and 16384 also build one alternative shape); get_schedule reports the shape in use. The
+ * autotuner (montmul_b200.tune) measures these per length and caches them. */
 typedef struct {
     int global;
     int launch_steps;
     double step_ns;
+    int threads;
 } mm_b200_schedule;
 int mm_b200_set_schedule(mm_b200_batch *b, const mm_b200_schedule *s);
 int mm_b200_get_schedule(const mm_b200_batch *b, mm_b200_schedule *s);

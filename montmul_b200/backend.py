@@ -65,6 +65,7 @@ SIGNATURES = {
     "mm_b200_wait_check": ([_vp, C.c_uint64], C.c_int),
     "mm_b200_run_items_async": ([_vp, _sz, _vp, _vp], C.c_int),
     "mm_b200_blocks_per_sm": ([_vp], C.c_int),
+    "mm_b200_busy": ([_vp], C.c_int),
     "mm_b200_bfly_peak": ([C.c_int, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)], C.c_int),
     "mm_b200_set_schedule": ([_vp, _vp], C.c_int),
     "mm_b200_get_schedule": ([_vp, _vp], C.c_int),
@@ -119,7 +120,7 @@ class TBuf:
 
 class Schedule(C.Structure):
     """mm_b200_schedule: global mode, steps per launch, measured ns per slot-step."""
-    _fields_ = [("global_", C.c_int), ("launch_steps", C.c_int), ("step_ns", C.c_double)]
+    _fields_ = [("global_", C.c_int), ("launch_steps", C.c_int), ("step_ns", C.c_double), ("threads", C.c_int)]
 
 
 def _ptr(a):
@@ -177,6 +178,7 @@ class B200:
         REDC (bit-identical to Cpu::with_wraparound); off, k = k0 and the plain REDC
         (bit-identical to Cpu::default)."""
         self.device = device
+        self.wraparound = bool(wraparound)
         opts = Options(device, int(force_global), int(wraparound), max_launch_steps)
         self._tuned = tuned and not max_launch_steps and not force_global
         self._table = None
@@ -228,9 +230,9 @@ class B200:
             from . import tune
             if self._table is None:
                 self._table = tune.load_table()
-            sc = tune.schedule_for(self.device_name(), length, self._table)
+            sc = tune.schedule_for(self.device_name(), length, self._table, self.wraparound)
             if sc:
-                self.set_schedule(st, sc["global"], sc["launch_steps"], sc["step_ns"])
+                self.set_schedule(st, sc["global"], sc["launch_steps"], sc["step_ns"], sc.get("block_threads", 0))
         return st
 
     def load(self, st, i, limbs):
@@ -281,6 +283,10 @@ class B200:
         t = np.ascontiguousarray(steps, np.uint32)
         assert s.size == t.size
         _check(lib().mm_b200_run_items_async(st.ptr, s.size, _ptr(s), _ptr(t)))
+
+    def busy(self, st) -> bool:
+        """True while work enqueued on the batch's stream is still running."""
+        return bool(lib().mm_b200_busy(st.ptr))
 
     def blocks_per_sm(self, st) -> int:
         """Blocks of the batch's step kernel one SM holds at once."""
@@ -354,18 +360,18 @@ class B200:
         return TBuf(ptr, length, count, self)
 
     # Schedules and in-place refill (no counterpart in the reference's Backend trait).
-    def set_schedule(self, st, global_mode, launch_steps: int = 0, step_ns: float = 0.0):
+    def set_schedule(self, st, global_mode, launch_steps: int = 0, step_ns: float = 0.0, threads: int = 0):
         """global_mode: 0 (or False) shared memory, 1 (or True) global mode, 2 cluster mode
         (L = 32768 and 65536: one thread-block cluster per slot, the vector in the cluster's
-        shared memory)."""
-        sc = Schedule(int(global_mode), int(launch_steps), float(step_ns))
+        shared memory). threads: threads per block of the shared-memory step (0: the default)."""
+        sc = Schedule(int(global_mode), int(launch_steps), float(step_ns), int(threads))
         _check(lib().mm_b200_set_schedule(st.ptr, C.byref(sc)))
 
     def get_schedule(self, st):
         sc = Schedule()
         _check(lib().mm_b200_get_schedule(st.ptr, C.byref(sc)))
         return {"global": bool(sc.global_), "mode": ("shared", "global", "cluster")[sc.global_],
-                "launch_steps": sc.launch_steps, "step_ns": sc.step_ns}
+                "launch_steps": sc.launch_steps, "step_ns": sc.step_ns, "threads": sc.threads}
 
     def set_moduli(self, st, slots, n, nprime):
         ids = np.ascontiguousarray(slots, np.uintp)

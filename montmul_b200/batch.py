@@ -201,20 +201,28 @@ class ModBatch:
         m = self.moduli[i]
         return gmp.mulmod(self.read_raw(i), m.rinv, m.n)
 
-    def refill(self, slots, moduli, xs, exps) -> None:
+    def prepare(self, n: int):
+        """The host set-up of modulus n for this batch's limb count (N', R mod N, R^-1 mod N, the
+        limb rows): what refill computes, done ahead, e.g. while the device runs."""
+        n = int(n)
+        if n <= 1 or n % 2 == 0:
+            raise MontMulError("modulus must be odd and > 1")
+        k = self.params.k
+        if Params.for_bits(n.bit_length(), self.backend.supported_lengths()).len > self.params.len or \
+                n.bit_length() + 4 > 32 * k:
+            raise MontMulError("modulus does not fit this batch's length")
+        return _setup_one(n, k)
+
+    def refill(self, slots, moduli, xs, exps, setups=None) -> None:
         """Replaces the moduli of `slots` and loads x and an exponent into each, the other slots
         keeping their state on the device (a serving loop's in-place refill; no counterpart in
-        the reference). Every new modulus must fit this batch's length and limb count."""
+        the reference). Every new modulus must fit this batch's length and limb count. `setups`
+        may carry each modulus's prepare() result, computed earlier."""
         slots = [int(i) for i in slots]
         moduli = [int(n) for n in moduli]
         k = self.params.k
-        for n in moduli:
-            if n <= 1 or n % 2 == 0:
-                raise MontMulError("modulus must be odd and > 1")
-            if Params.for_bits(n.bit_length(), self.backend.supported_lengths()).len > self.params.len or \
-                    n.bit_length() + 4 > 32 * k:
-                raise MontMulError("modulus does not fit this batch's length")
-        per = [_setup_one(n, k) for n in moduli]
+        per = [s if s is not None and s[3].n == n else self.prepare(n)
+               for n, s in zip(moduli, setups if setups is not None else [None] * len(moduli))]
         self.backend.set_moduli(self.state, slots, np.stack([p[0] for p in per]), np.stack([p[1] for p in per]))
         for i, p in zip(slots, per):
             self.moduli[i] = p[3]

@@ -35,6 +35,8 @@ typedef void (*TransformFn)(F2*, F1*, const F2K*, const F1*, uint32_t, int);
 
 struct KernelSet {
     StepFn step;
+    StepFn step_alt;         // the alternative block shape of this length's step (nullptr: none)
+    int threads_alt;
     MulFn mul;
     SetupFn setup;
     TransformFn transform;   // the Transform trait's forward / inverse (shared memory)
@@ -81,6 +83,8 @@ struct MixedDesc {
     GArgs g;        // the batch's slot state (w2 / w1 unused in shared mode)
     int global;     // 1: global mode; 0: the vector in shared memory
     uint32_t bits;  // steps per item of this batch in this launch (0: the launch's `bits`)
+    const F2K* ctab2;   // cluster items: the shared-layout tables of the batch's length
+    const F1* ctab1;
 };
 constexpr int kMixedThreads = 256;        // one group: the threads on one slot
 constexpr int kMixedGroups = 2;           // groups per block (gsync has barriers for two)
@@ -93,16 +97,27 @@ constexpr int kWideThreads = kMixedBlockThreads;
 static_assert(kMixedSmem == (24 << kWideLogN), "one wide vector fills the groups' shared memory");
 // Items: (descriptor, slot, steps, unused); steps 0 takes the descriptor's, then the launch's.
 // The item counts are read from device memory, so one captured launch serves any lists.
-// counter[0] counts the group items taken, counter[1] the wide items.
+// counter[0] counts the group items taken, counter[1] the wide items, counter[2] the cluster
+// items. The launch is a cluster launch of block pairs (kMixedCluster): each pair first takes
+// cluster items (L = 32768 batches in cluster mode, the pair on one slot, mm_cluster.cuh), then
+// its blocks go on independently.
+constexpr int kMixedCluster = 2;
+constexpr int kPairLogN = 14;
 struct MixedLists {
     const uint4* items;
     const uint32_t* count;
     const uint4* wide;
     const uint32_t* wide_count;
     uint32_t* counter;
+    const uint4* pair;            // cluster items (L = 32768 in cluster mode): a block pair each
+    const uint32_t* pair_count;
 };
 typedef void (*MixedFn)(const MixedDesc*, MixedLists, uint32_t);
 MixedFn mixed_kernel();               // mm_mixed.cu
+// The mixed launch on a stream: a cluster launch of `grid` blocks (pairs), grid a multiple of
+// kMixedCluster; returns a cudaError_t value. mixed_clusters gives the pairs that fit at once.
+int mixed_launch(int grid, const MixedDesc* descs, const MixedLists& l, uint32_t bits, void* stream);
+int mixed_clusters(int* clusters);
 
 // Threads per block for transform length 2^m: one radix-8 group per thread up to 256 threads;
 // n = 8192 (one block per SM, all of its shared memory) takes 512, which hide more latency.
@@ -112,6 +127,11 @@ MixedFn mixed_kernel();               // mm_mixed.cu
 constexpr int threads_for(int m) {
     return m >= kWideLogN || m == 12 ? 512 : (m - 3 <= 5 ? 32 : (m - 3 >= 8 ? 256 : (1 << (m - 3))));
 }
+
+// The alternative step-kernel shape a schedule may select per length (threads, minimum blocks per
+// SM; 0 threads: none): the runner-up of the shapes measured at full occupancy, 4,096 <= L <= 16,384.
+constexpr int alt_threads_for(int m) { return m == 11 ? 256 : (m == 12 ? 256 : (m == 13 ? 1024 : 0)); }
+constexpr int alt_min_blocks_for(int m) { return m == 11 ? 4 : (m == 12 ? 2 : 1); }
 
 // Defined in mm_inst.cu for each m in [kMinLogN, kMaxSharedLogN].
 #define MM_DECLARE_KERNELS(M) KernelSet kernels_m##M();

@@ -88,6 +88,8 @@ struct mm_b200_batch {
     size_t k = 0, n = 0, slots = 0;
     uint32_t base = 3;
     KernelSet ks{};
+    StepFn step_fn = nullptr;  // the step kernel of the schedule's block shape (ks.step or ks.step_alt)
+    int step_threads = 0;
     bool global = false;       // vector in HBM, tiles through shared memory (mm_global.cuh)
     bool cluster = false;      // global batch stepped in cluster mode (mm_cluster.cuh)
     const DevTables* ctab = nullptr;   // shared-layout tables of a cluster-mode length
@@ -96,10 +98,11 @@ struct mm_b200_batch {
     F2* d_w2 = nullptr;        // global mode: slots x n work elements
     F1* d_w1 = nullptr;
     const DevTables* gtab = nullptr;   // global-mode tables (global batches)
-    mm_b200_schedule sched{0, 0, 0.0};
+    mm_b200_schedule sched{0, 0, 0.0, 0};
     uint32_t* d_stage = nullptr;       // refill staging: device words and pinned host words
     size_t stage_cap = 0;
     uint32_t* h_stage = nullptr;
+    cudaEvent_t stage_copied = nullptr;   // the last host-to-device copy out of h_stage
     size_t hstage_cap = 0;
     cudaStream_t stream = nullptr;
     uint32_t* d_x = nullptr;
@@ -166,6 +169,11 @@ int ensure_tables(mm_b200_device* dev, int m, bool global, const DevTables** out
         MM_CK(cudaFuncSetAttribute((const void*)ks.transform, cudaFuncAttributeMaxDynamicSharedMemorySize, ks.smem));
         MM_CK(cudaFuncSetAttribute((const void*)ks.step, cudaFuncAttributePreferredSharedMemoryCarveout,
                                    cudaSharedmemCarveoutMaxShared));
+        if (ks.step_alt) {
+            MM_CK(cudaFuncSetAttribute((const void*)ks.step_alt, cudaFuncAttributeMaxDynamicSharedMemorySize, ks.smem));
+            MM_CK(cudaFuncSetAttribute((const void*)ks.step_alt, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                       cudaSharedmemCarveoutMaxShared));
+        }
         dev->configured[m] = true;
     }
     *out = &it->second;
@@ -296,7 +304,7 @@ int launch_steps(mm_b200_batch* b, size_t bits, bool bare = false) {
         } else if (b->global) {
             b->gk.step<<<(unsigned)b->slots, b->gk.threads, b->gk.smem, b->stream>>>(g, 0, s);
         } else {
-            b->ks.step<<<(unsigned)b->slots, b->ks.threads, b->ks.smem, b->stream>>>(a, 0, s, nullptr);
+            b->step_fn<<<(unsigned)b->slots, b->step_threads, b->ks.smem, b->stream>>>(a, 0, s, nullptr);
         }
         MM_CK(cudaGetLastError());
         ++b->launches;
@@ -344,6 +352,13 @@ int ensure_cluster(mm_b200_batch* b) {
 // Staging words for a refill: pinned host and device buffers of at least `words` u32. Waits
 // for the batch's stream first, since an earlier copy may still read the pinned buffer.
 int ensure_stage(mm_b200_batch* b, size_t words) {
+    if (!b->stage_copied) MM_CK(cudaEventCreateWithFlags(&b->stage_copied, cudaEventDisableTiming));
+    if (words <= b->stage_cap && words <= b->hstage_cap) {
+        // The pinned words may be rewritten once the last copy out of them has passed; device
+        // work that still reads the device staging is ordered before the next copy by the stream.
+        MM_CK(cudaEventSynchronize(b->stage_copied));
+        return MM_OK;
+    }
     MM_CK(cudaStreamSynchronize(b->stream));
     if (words > b->stage_cap) {
         if (b->d_stage) MM_CK(cudaFree(b->d_stage));
@@ -564,8 +579,13 @@ int mm_b200_create(mm_b200_device* dev, size_t k, size_t len, uint32_t base, siz
     b->plain = !dev->wrap;
     b->sched.global = global ? 1 : 0;
     b->gk = global_kernels();
+    b->sched.threads = global ? b->gk.threads : (m <= kMaxSharedLogN ? threads_for(m) : 0);
     b->gtab = gtab;
-    if (m <= kMaxSharedLogN) kernel_set(m, b->ks);
+    if (m <= kMaxSharedLogN) {
+        kernel_set(m, b->ks);
+        b->step_fn = b->ks.step;
+        b->step_threads = b->ks.threads;
+    }
     MM_CK(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
     const size_t nn = b->n;
     MM_CK(cudaMalloc(&b->d_x, slots * k * 4));
@@ -743,7 +763,7 @@ int mm_b200_run_items_async(mm_b200_batch* b, size_t count, const size_t* slots,
     SlotArgs a = slot_args(b);
     for (size_t first = 0; first < count; first += 65535) {
         const unsigned grid = (unsigned)std::min<size_t>(65535, count - first);
-        b->ks.step<<<grid, b->ks.threads, b->ks.smem, b->stream>>>(a, 0, 0, b->d_items + first);
+        b->step_fn<<<grid, b->step_threads, b->ks.smem, b->stream>>>(a, 0, 0, b->d_items + first);
         MM_CK(cudaGetLastError());
         ++b->launches;
     }
@@ -755,12 +775,19 @@ int mm_b200_run_items_async(mm_b200_batch* b, size_t count, const size_t* slots,
     return MM_OK;
 }
 
+int mm_b200_busy(const mm_b200_batch* b) {
+    if (!b) return 0;
+    if (cudaSetDevice(b->dev->device) != cudaSuccess) return 0;
+    const cudaError_t e = cudaStreamQuery(b->stream);
+    return e == cudaErrorNotReady ? 1 : 0;
+}
+
 int mm_b200_blocks_per_sm(const mm_b200_batch* b) {
     if (!b) return 0;
     int per = 0;
     if (b->cluster || b->global) return b->cluster ? 1 : 2;
     if (cudaSetDevice(b->dev->device) != cudaSuccess) return 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, b->ks.step, b->ks.threads, b->ks.smem) != cudaSuccess) return 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, b->step_fn, b->step_threads, b->ks.smem) != cudaSuccess) return 0;
     return per;
 }
 
@@ -817,6 +844,7 @@ void mm_b200_destroy(mm_b200_batch* b) {
     cudaFree(b->d_w1);
     cudaFree(b->d_stage);
     if (b->h_stage) cudaFreeHost(b->h_stage);
+    if (b->stage_copied) cudaEventDestroy(b->stage_copied);
     if (b->stream) cudaStreamDestroy(b->stream);
     if (b->host_x) cudaFreeHost(b->host_x);
     if (b->host_exp) cudaFreeHost(b->host_exp);
@@ -837,6 +865,17 @@ int mm_b200_set_schedule(mm_b200_batch* b, const mm_b200_schedule* sc) {
     if (cluster && (b->m < kMinClusterLogN || b->m > kMaxClusterLogN))
         return fail(MM_ERR_UNSUPPORTED, "set_schedule: cluster mode runs L = 32768 and 65536 only");
     if (cluster && b->plain) return fail(MM_ERR_UNSUPPORTED, "set_schedule: cluster mode needs the wraparound path");
+    StepFn fn = b->ks.step;
+    int threads = b->ks.threads;
+    if (!global && sc->threads != 0 && sc->threads != b->ks.threads) {
+        if (!b->ks.step_alt || sc->threads != b->ks.threads_alt)
+            return fail(MM_ERR_UNSUPPORTED, "set_schedule: L = " + std::to_string(2 * b->n) + " runs " +
+                                                std::to_string(b->ks.threads) +
+                                                (b->ks.step_alt ? " or " + std::to_string(b->ks.threads_alt) : std::string()) +
+                                                " threads per block");
+        fn = b->ks.step_alt;
+        threads = b->ks.threads_alt;
+    }
     if (global) {
         int rc = ensure_global_buffers(b);
         if (rc) return rc;
@@ -847,8 +886,13 @@ int mm_b200_set_schedule(mm_b200_batch* b, const mm_b200_schedule* sc) {
     }
     b->global = global;
     b->cluster = cluster;
+    if (!global) {
+        b->step_fn = fn;
+        b->step_threads = threads;
+    }
     b->sched = *sc;
     b->sched.global = cluster ? 2 : (global ? 1 : 0);
+    b->sched.threads = global ? (cluster ? 512 : b->gk.threads) : threads;
     return MM_OK;
 }
 
@@ -871,6 +915,7 @@ int mm_b200_set_moduli(mm_b200_batch* b, size_t count, const size_t* slots, cons
     std::memcpy(h + count, n, count * k * 4);
     std::memcpy(h + count + count * k, nprime, count * k * 4);
     MM_CK(cudaMemcpyAsync(b->d_stage, h, count * (1 + 2 * k) * 4, cudaMemcpyHostToDevice, b->stream));
+    MM_CK(cudaEventRecord(b->stage_copied, b->stream));
     const DevTables* tab = b->global ? b->gtab : b->tab;
     for (size_t c0 = 0; c0 < count; c0 += 65535) {
         const unsigned grid = (unsigned)std::min<size_t>(65535, count - c0);
@@ -919,6 +964,7 @@ int mm_b200_write_slots(mm_b200_batch* b, size_t count, const size_t* slots, con
     if (x) std::memcpy(h + 2 * count, x, count * k * 4);
     if (words) std::memcpy(h + 2 * count + count * k, words, count * ew * 4);
     MM_CK(cudaMemcpyAsync(b->d_stage, h, total * 4, cudaMemcpyHostToDevice, b->stream));
+    MM_CK(cudaEventRecord(b->stage_copied, b->stream));
     scatter_rows_kernel<<<(unsigned)count, 128, 0, b->stream>>>(b->d_stage, (uint32_t)count, (uint32_t)k, (uint32_t)ewi,
                                                                 (uint32_t)b->ew, x ? b->d_x : nullptr,
                                                                 words ? b->d_exp : nullptr, b->d_nbits, b->d_pos);
@@ -950,6 +996,7 @@ int mm_b200_read_slots(mm_b200_batch* b, size_t count, const size_t* slots, uint
     uint32_t* h = b->h_stage;
     for (size_t r = 0; r < count; ++r) h[r] = (uint32_t)slots[r];
     MM_CK(cudaMemcpyAsync(b->d_stage, h, count * 4, cudaMemcpyHostToDevice, b->stream));
+    MM_CK(cudaEventRecord(b->stage_copied, b->stream));
     gather_rows_kernel<<<(unsigned)count, 128, 0, b->stream>>>(b->d_stage, (uint32_t)k, b->d_x, b->d_stage + count);
     MM_CK(cudaGetLastError());
     MM_CK(cudaMemcpyAsync(h + count, b->d_stage + count, count * k * 4, cudaMemcpyDeviceToHost, b->stream));
@@ -964,7 +1011,7 @@ int mm_b200_read_slots(mm_b200_batch* b, size_t count, const size_t* slots, uint
 struct mm_b200_plan {
     mm_b200_device* dev = nullptr;
     std::vector<mm_b200_batch*> batches;
-    std::vector<char> wide;           // per batch: its slots are in d_wide (its kind at creation)
+    std::vector<char> wide;           // per batch: 1 its slots are in d_wide, 2 in d_pair (its kind at creation)
     std::vector<cudaEvent_t> ready;   // per batch: its stream's work before a launch
     cudaEvent_t done = nullptr;       // the plan's last launch
     cudaStream_t stream = nullptr;
@@ -975,10 +1022,12 @@ struct mm_b200_plan {
     // Every slot (plan_run, plan_run_each): the group items longest first, then the wide items.
     uint4* d_items = nullptr;
     uint4* d_wide = nullptr;
+    uint4* d_pair = nullptr;           // cluster items (a block pair on one slot)
     uint32_t count = 0;                // slots of all batches
-    // [0], [1]: counts of d_items and d_wide; [2], [3]: counts of plan_run_items' two lists.
+    // [0], [1], [2]: counts of d_items, d_wide and d_pair; [3], [4], [5]: counts of
+    // plan_run_items' three lists.
     uint32_t* d_count = nullptr;
-    uint4* d_tick = nullptr;           // plan_run_items' lists: group items at 0, wide at `count`
+    uint4* d_tick = nullptr;           // plan_run_items' lists: group items at 0, wide at `count`, pairs at 2 `count`
     uint4* h_tick = nullptr;           // pinned staging of those lists (+ their counts)
     cudaGraph_t graph_items = nullptr;
     cudaGraphExec_t exec_items = nullptr;
@@ -1011,6 +1060,8 @@ MixedDesc mixed_desc(const mm_b200_batch* b, bool global, uint32_t bits) {
         d.g.m = b->m;
     }
     d.global = global ? 1 : 0;
+    d.ctab2 = b->ctab ? b->ctab->t2 : nullptr;
+    d.ctab1 = b->ctab ? b->ctab->t1 : nullptr;
     return d;
 }
 
@@ -1018,15 +1069,19 @@ MixedDesc mixed_desc(const mm_b200_batch* b, bool global, uint32_t bits) {
 bool plan_wide(const mm_b200_batch* b) { return !b->global && b->m == kWideLogN; }
 // A batch whose slots run in global mode inside the mixed launch.
 bool plan_global(const mm_b200_batch* b) { return b->global || b->m > kWideLogN; }
+// A batch whose slots run as cluster items (a block pair each, mm_cluster.cuh): L = 32768 in
+// cluster mode.
+bool plan_pair(const mm_b200_batch* b) { return b->cluster && b->m == kPairLogN && b->ctab && !b->plain; }
+int plan_kind(const mm_b200_batch* b) { return plan_pair(b) ? 2 : (plan_wide(b) ? 1 : 0); }
 
-// The counter reset and one persistent launch over lists `items` (count at count[0]) and `wide`
-// (count at count[1]).
-cudaError_t plan_launch(mm_b200_plan* p, const uint4* items, const uint4* wide, const uint32_t* count, uint32_t bits) {
-    cudaError_t e = cudaMemsetAsync(p->d_counter, 0, 2 * sizeof(uint32_t), p->stream);
+// The counter reset and one persistent launch over lists `items` (count at count[0]), `wide`
+// (count at count[1]) and `pair` (count at count[2]).
+cudaError_t plan_launch(mm_b200_plan* p, const uint4* items, const uint4* wide, const uint4* pair, const uint32_t* count,
+                        uint32_t bits) {
+    cudaError_t e = cudaMemsetAsync(p->d_counter, 0, 3 * sizeof(uint32_t), p->stream);
     if (e != cudaSuccess) return e;
-    const MixedLists l{items, count, wide, count + 1, p->d_counter};
-    mixed_kernel()<<<p->grid, kMixedBlockThreads, kMixedSmem, p->stream>>>(p->d_descs, l, bits);
-    return cudaGetLastError();
+    const MixedLists l{items, count, wide, count + 1, p->d_counter, pair, count + 2};
+    return (cudaError_t)mixed_launch(p->grid, p->d_descs, l, bits, p->stream);
 }
 
 // Descriptor of batch i for plan_run and plan_run_each, whose item lists were built at creation:
@@ -1036,12 +1091,12 @@ cudaError_t plan_launch(mm_b200_plan* p, const uint4* items, const uint4* wide, 
 // the same in both modes, so the results do not depend on the mode.
 MixedDesc plan_desc(const mm_b200_plan* p, size_t i, uint32_t bits) {
     const mm_b200_batch* b = p->batches[i];
-    return mixed_desc(b, !p->wide[i] && (plan_global(b) || b->m == kWideLogN), bits);
+    return mixed_desc(b, p->wide[i] != 1 && (plan_global(b) || b->m == kWideLogN), bits);
 }
 
 // One launch of `bits` steps over every slot.
 int plan_enqueue(mm_b200_plan* p, uint32_t bits) {
-    MM_CK(plan_launch(p, p->d_items, p->d_wide, p->d_count, bits));
+    MM_CK(plan_launch(p, p->d_items, p->d_wide, p->d_pair, p->d_count, bits));
     return MM_OK;
 }
 
@@ -1071,7 +1126,7 @@ int mm_b200_plan_create(mm_b200_batch* const* batches, size_t count, size_t quan
     p->dev = dev;
     p->batches.assign(batches, batches + count);
     p->wide.assign(count, 0);
-    for (size_t i = 0; i < count; ++i) p->wide[i] = plan_wide(batches[i]) ? 1 : 0;
+    for (size_t i = 0; i < count; ++i) p->wide[i] = (char)plan_kind(batches[i]);
     p->quantum = quantum;
     p->count = (uint32_t)total;
     MM_CK(cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking));
@@ -1087,20 +1142,25 @@ int mm_b200_plan_create(mm_b200_batch* const* batches, size_t count, size_t quan
             dev->mixed_configured = true;
         }
     }
-    int per_sm = 0;
-    MM_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, mixed_kernel(), kMixedBlockThreads, kMixedSmem));
-    if (per_sm < 1) return fail(MM_ERR_CUDA, "plan_create: the mixed launch fits no block on an SM");
-    p->grid = per_sm * dev->sms;
+    // Block pairs that fit on the device at once (the launch is a cluster launch of pairs).
+    int pairs = 0;
+    {
+        const int e = mixed_clusters(&pairs);
+        if (e) return fail(MM_ERR_CUDA, std::string("plan_create: ") + cudaGetErrorString((cudaError_t)e));
+    }
+    if (pairs < 1) return fail(MM_ERR_CUDA, "plan_create: the mixed launch fits no block pair on the device");
+    p->grid = pairs * kMixedCluster;
     // Group items longest first (by cost per step; every slot of a batch has the same), then by
-    // batch and slot; wide items by batch and slot.
+    // batch and slot; wide and cluster items by batch and slot.
     std::vector<std::pair<double, uint4>> items;
-    std::vector<uint4> wide;
+    std::vector<uint4> wide, pair;
     items.reserve(total);
     for (size_t i = 0; i < count; ++i) {
         const double c = step_cost(batches[i], plan_global(batches[i]));
         for (size_t s = 0; s < batches[i]->slots; ++s) {
             const uint4 it = make_uint4((unsigned)i, (unsigned)s, 0u, 0u);
-            if (p->wide[i]) wide.push_back(it);
+            if (p->wide[i] == 2) pair.push_back(it);
+            else if (p->wide[i] == 1) wide.push_back(it);
             else items.push_back({c, it});
         }
     }
@@ -1108,16 +1168,18 @@ int mm_b200_plan_create(mm_b200_batch* const* batches, size_t count, size_t quan
     std::vector<uint4> it(total);
     for (size_t i = 0; i < items.size(); ++i) it[i] = items[i].second;
     std::copy(wide.begin(), wide.end(), it.begin() + items.size());
+    std::copy(pair.begin(), pair.end(), it.begin() + items.size() + wide.size());
     MM_CK(cudaMalloc(&p->d_items, total * sizeof(uint4)));
     MM_CK(cudaMemcpy(p->d_items, it.data(), total * sizeof(uint4), cudaMemcpyHostToDevice));
     p->d_wide = p->d_items + items.size();
-    MM_CK(cudaMalloc(&p->d_count, 4 * sizeof(uint32_t)));
-    const uint32_t counts[4] = {(uint32_t)items.size(), (uint32_t)wide.size(), 0, 0};
+    p->d_pair = p->d_wide + wide.size();
+    MM_CK(cudaMalloc(&p->d_count, 6 * sizeof(uint32_t)));
+    const uint32_t counts[6] = {(uint32_t)items.size(), (uint32_t)wide.size(), (uint32_t)pair.size(), 0, 0, 0};
     MM_CK(cudaMemcpy(p->d_count, counts, sizeof(counts), cudaMemcpyHostToDevice));
     MM_CK(cudaMalloc(&p->d_descs, count * sizeof(MixedDesc)));
     MM_CK(cudaMallocHost(&p->h_descs, count * sizeof(MixedDesc)));
     std::memset(p->h_descs, 0, count * sizeof(MixedDesc));
-    MM_CK(cudaMalloc(&p->d_counter, 2 * sizeof(uint32_t)));
+    MM_CK(cudaMalloc(&p->d_counter, 3 * sizeof(uint32_t)));
     *out = p.release();
     return MM_OK;
 }
@@ -1265,26 +1327,33 @@ int mm_b200_plan_run_items(mm_b200_plan* p, size_t count, const uint32_t* batch,
     }
     const size_t cap = p->count;
     if (!p->d_tick) {
-        MM_CK(cudaMalloc(&p->d_tick, 2 * cap * sizeof(uint4)));
-        MM_CK(cudaMallocHost(&p->h_tick, (2 * cap + 1) * sizeof(uint4)));
+        MM_CK(cudaMalloc(&p->d_tick, 3 * cap * sizeof(uint4)));
+        MM_CK(cudaMallocHost(&p->h_tick, (3 * cap + 1) * sizeof(uint4)));
     }
-    // The list splits into group items (in list order) at 0 and wide items (in list order) at cap.
-    size_t ng = 0, nw = 0;
+    // The list splits into group items at 0, wide items at cap and cluster items at 2 cap, each
+    // in list order; a batch keeps the kind it has now.
+    size_t ng = 0, nw = 0, np = 0;
     for (size_t i = 0; i < count; ++i) {
         const uint4 it = make_uint4(batch[i], slot[i], steps[i], 0u);
-        if (plan_wide(p->batches[batch[i]])) p->h_tick[cap + nw++] = it;
+        const int kind = plan_kind(p->batches[batch[i]]);
+        if (kind == 2) p->h_tick[2 * cap + np++] = it;
+        else if (kind == 1) p->h_tick[cap + nw++] = it;
         else p->h_tick[ng++] = it;
     }
-    uint32_t* hc = reinterpret_cast<uint32_t*>(p->h_tick + 2 * cap);
+    uint32_t* hc = reinterpret_cast<uint32_t*>(p->h_tick + 3 * cap);
     hc[0] = (uint32_t)ng;
     hc[1] = (uint32_t)nw;
+    hc[2] = (uint32_t)np;
     if (ng) MM_CK(cudaMemcpyAsync(p->d_tick, p->h_tick, ng * sizeof(uint4), cudaMemcpyHostToDevice, p->stream));
     if (nw)
         MM_CK(cudaMemcpyAsync(p->d_tick + cap, p->h_tick + cap, nw * sizeof(uint4), cudaMemcpyHostToDevice, p->stream));
-    MM_CK(cudaMemcpyAsync(p->d_count + 2, hc, 2 * sizeof(uint32_t), cudaMemcpyHostToDevice, p->stream));
+    if (np)
+        MM_CK(cudaMemcpyAsync(p->d_tick + 2 * cap, p->h_tick + 2 * cap, np * sizeof(uint4), cudaMemcpyHostToDevice,
+                              p->stream));
+    MM_CK(cudaMemcpyAsync(p->d_count + 3, hc, 3 * sizeof(uint32_t), cudaMemcpyHostToDevice, p->stream));
     if (!p->exec_items) {
         MM_CK(cudaStreamBeginCapture(p->stream, cudaStreamCaptureModeThreadLocal));
-        const cudaError_t e0 = plan_launch(p, p->d_tick, p->d_tick + cap, p->d_count + 2, 0);
+        const cudaError_t e0 = plan_launch(p, p->d_tick, p->d_tick + cap, p->d_tick + 2 * cap, p->d_count + 3, 0);
         cudaGraph_t g = nullptr;
         cudaError_t e = cudaStreamEndCapture(p->stream, &g);
         if (e0 != cudaSuccess) return fail(MM_ERR_CUDA, std::string("plan capture: ") + cudaGetErrorString(e0));

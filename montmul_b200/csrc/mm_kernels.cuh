@@ -280,8 +280,8 @@ __device__ __forceinline__ void step_slot(const SlotArgs& a, uint32_t slot, uint
 // The uniform launch: one block per slot first + blockIdx.x, `bits` steps each; or, with an item
 // list, one block per item (slot, steps) of the list (a serving tick's launch over the busy slots
 // of a batch; each slot at most once).
-template <int M, int NT>
-__global__ void __launch_bounds__(NT, (M <= 12 ? 2 : 1))
+template <int M, int NT, int MINB = (M <= 12 ? 2 : 1)>
+__global__ void __launch_bounds__(NT, MINB)
     step_kernel(SlotArgs a, uint32_t first, uint32_t bits, const uint2* __restrict__ items) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ uint64_t sc[CarryScratch<NT>::words];

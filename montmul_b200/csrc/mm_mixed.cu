@@ -4,14 +4,16 @@
 // takes the next item; the host orders the items longest first, which bounds the tail of the
 // launch by the cost of one of the shortest items.
 //
-// One block per SM: 512 threads and 192 KiB of dynamic shared memory. The block first takes the
-// wide items (L = 16384 in shared mode: all 512 threads and all of the shared memory on one
+// One block per SM: 512 threads and 192 KiB of dynamic shared memory, launched as clusters of two
+// blocks. Each pair first takes the cluster items (L = 32768 batches in cluster mode: the pair
+// on one slot, the vector in the two blocks' shared memory, mm_cluster.cuh). Each block then
+// takes the wide items (L = 16384 in shared mode: all 512 threads and all of the shared memory on one
 // slot), then splits into two groups of 256 threads, each with its own 96 KiB and hardware
 // barrier, which take the other items independently: lengths with n <= 4096 with the whole
 // vector in shared memory, longer ones (and batches tuned to it) in global mode. There is no
 // counterpart in the reference, whose launches each cover one batch of one length
 // (montmul/src/gpu/mod.rs:119-158).
-#include "mm_global.cuh"
+#include "mm_cluster.cuh"
 
 namespace mm {
 
@@ -28,9 +30,17 @@ __device__ __noinline__ void mixed_wide(const SlotArgs& a, uint32_t slot, uint32
     step_slot<kWideLogN, kWideThreads>(a, slot, bits, smem, sc);
 }
 
+__device__ __noinline__ void mixed_pair(const SlotArgs& a, uint32_t slot, uint32_t bits, unsigned char* smem,
+                                        uint64_t* sc, ClusterCarry* cc) {
+    cl_step_slot<kPairLogN, kWideThreads, kMixedCluster>(a, slot, bits, smem, sc, cc);
+}
+
 // gsync / gsync_or (mm_ntt.cuh) give a block at most two groups, and treat a group of 512 or
 // more threads as the whole block.
 static_assert(kMixedGroups == 2 && kWideThreads == 512, "group barriers: two workers, one wide group");
+static_assert(kWideThreads == kClusterThreads && kMixedSmem == kClusterSmem &&
+                  (1 << (kPairLogN - kChunkLog)) == kMixedCluster,
+              "a block pair holds one cluster item");
 
 constexpr int kGroupScratch = CarryScratch<kMixedThreads>::words;
 constexpr int kScratchWords = cmax(kMixedGroups * kGroupScratch, CarryScratch<kWideThreads>::words);
@@ -45,6 +55,28 @@ __global__ void __launch_bounds__(kMixedBlockThreads, 1)
     __shared__ uint64_t sc[kScratchWords];
     __shared__ uint64_t bars[kMixedGroups][2];
     __shared__ uint32_t next[kMixedGroups];
+    __shared__ uint32_t pair_next;
+    __shared__ ClusterCarry cc;
+    // Cluster items: the block pair on one slot. Block 0 of the pair takes the item and hands its
+    // index to block 1, so both leave the loop together.
+    const cgx::cluster_group cl = cgx::this_cluster();
+    const uint32_t pair_count = *l.pair_count;
+    while (pair_count) {
+        if (cl.block_rank() == 0 && threadIdx.x == 0) {
+            const uint32_t i = atomicAdd(&l.counter[2], 1u);
+            for (int d = 0; d < kMixedCluster; ++d) *cl.map_shared_rank(&pair_next, d) = i;
+        }
+        cl.sync();
+        const uint32_t i = pair_next;
+        cl.sync();   // every thread of the pair has read the index before it is replaced
+        if (i >= pair_count) break;
+        const uint4 it = l.pair[i];
+        const MixedDesc& d = descs[it.x];
+        SlotArgs a = d.g.a;
+        a.tab2 = d.ctab2;
+        a.tab1 = d.ctab1;
+        mixed_pair(a, it.y, item_steps(it, d, bits), smem_raw, sc, &cc);
+    }
     // Wide items: the whole block on one slot.
     const uint32_t wide_count = *l.wide_count;
     while (wide_count) {
@@ -96,5 +128,36 @@ __global__ void __launch_bounds__(kMixedBlockThreads, 1)
 }
 
 MixedFn mixed_kernel() { return mixed_step_kernel; }
+
+int mixed_launch(int grid, const MixedDesc* descs, const MixedLists& l, uint32_t bits, void* stream) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)grid, 1, 1);
+    cfg.blockDim = dim3(kMixedBlockThreads, 1, 1);
+    cfg.dynamicSmemBytes = kMixedSmem;
+    cfg.stream = static_cast<cudaStream_t>(stream);
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = kMixedCluster;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return (int)cudaLaunchKernelEx(&cfg, mixed_step_kernel, descs, l, bits);
+}
+
+int mixed_clusters(int* clusters) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(kMixedCluster, 1, 1);
+    cfg.blockDim = dim3(kMixedBlockThreads, 1, 1);
+    cfg.dynamicSmemBytes = kMixedSmem;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = kMixedCluster;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return (int)cudaOccupancyMaxActiveClusters(clusters, (const void*)mixed_step_kernel, &cfg);
+}
 
 }  // namespace mm

@@ -61,6 +61,7 @@ class Request:
     verdict: Optional[bool] = None
     value: Optional[int] = None
     raw: Optional[int] = None
+    setup: Optional[tuple] = None   # the modulus's host set-up, computed while the device runs
 
 
 def fixture_offsets(seed: int, lo: int, hi: int, prime_frac: float, mul_frac: float,
@@ -132,13 +133,15 @@ class Segment:
     batch: ModBatch
     free: list
     active: dict = field(default_factory=dict)   # slot -> Request
+    inflight: bool = False                       # a launch of this segment is on the device
 
 
 class Server:
     """Lanes of segments per transform length, one plan over every segment."""
 
     def __init__(self, dev, base: int = 3, quantum: int = 128, segment_slots: int = 0, budget_frac: float = 0.5,
-                 tuned: bool = True, checker: Optional["VerdictChecker"] = None):
+                 tuned: bool = True, checker: Optional["VerdictChecker"] = None, launch: str = "stream",
+                 slice_ms: float = 30.0):
         from .backend import lib
         self.dev = dev
         self.lib = lib()
@@ -160,6 +163,14 @@ class Server:
         self.table = tune.load_table().get(dev.device_name(), {})
         self.seg_steps = []       # per plan batch: steps of one tick
         self.checker = checker    # receives every finished Fermat request
+        if launch not in ("items", "plan", "stream"):
+            raise MontMulError("launch must be 'items', 'plan' or 'stream'")
+        self.launch = launch      # stream, items (ticks of per-segment launches) or plan (ticks of one mixed launch)
+        self.slice_ms = slice_ms  # stream mode: device time one launch of a segment is budgeted
+        self.sms = dev.sm_count()
+        self.bps = {}             # length -> blocks of its step kernel per SM
+        self.waiting = deque()    # requests waiting for a slot (serve() sets the live queue)
+        self.last_tick_s = 0.0
 
     # ---- admission ----
     def _grow(self, length: int) -> Optional[Segment]:
@@ -185,10 +196,16 @@ class Server:
         return seg
 
     def _slots_for(self, length: int, count: int):
-        """`count` free slots of one segment of the lane, growing the lane if needed."""
-        for seg in self.lanes.get(length, []):
-            if len(seg.free) >= count:
+        """`count` free slots of one segment of the lane that has no launch on the device. When
+        only segments with a launch in flight have room, the request waits for one of them to
+        finish (a refill cannot race the running launch); the lane grows only when no segment
+        has room."""
+        segs = self.lanes.get(length, [])
+        for seg in segs:
+            if not seg.inflight and len(seg.free) >= count:
                 return seg, [seg.free.pop() for _ in range(count)]
+        if any(len(seg.free) >= count for seg in segs):
+            return None, None
         seg = self._grow(length)
         if seg is None or len(seg.free) < count:
             return None, None
@@ -217,9 +234,26 @@ class Server:
             e[2].append(r)
         waiting.extend(kept)
         for seg, slots, reqs in fermat.values():
-            seg.batch.refill(slots, [r.n for r in reqs], [1] * len(reqs), [r.n - 1 for r in reqs])
+            seg.batch.refill(slots, [r.n for r in reqs], [1] * len(reqs), [r.n - 1 for r in reqs],
+                             [r.setup for r in reqs])
             for s, r in zip(slots, reqs):
                 seg.active[s] = r
+                r.setup = None
+
+    def prepare(self, waiting, budget_s: float) -> None:
+        """Host set-up of waiting requests (GMP: N', R mod N, R^-1 mod N) ahead of their
+        admission, oldest first, for about `budget_s` seconds: done while the device runs a tick."""
+        t_end = time.perf_counter() + budget_s
+        for r in waiting:
+            if time.perf_counter() > t_end:
+                break
+            if r.setup is not None or r.kind != "fermat":
+                continue
+            if not r.length:
+                r.length = Params.for_bits(r.n.bit_length(), self.lengths).len
+            seg = next(iter(self.lanes.get(r.length, [])), None)
+            if seg is not None:
+                r.setup = seg.batch.prepare(r.n)
 
     def _mul(self, seg: Segment, slots, r: Request) -> None:
         b = seg.batch
@@ -297,17 +331,70 @@ class Server:
     def busy(self) -> int:
         return sum(len(s.active) for segs in self.lanes.values() for s in segs)
 
+    def item_lat_ns(self, seg: Segment) -> float:
+        """Time one busy slot of a segment's length takes per step while the GPU is full of its
+        length: the uniform kernel's GPU time per slot-step times the slots resident at once."""
+        length = seg.batch.params.len
+        if length not in self.bps:
+            be, st = seg.batch.backend_and_state()
+            self.bps[length] = max(1, be.blocks_per_sm(st))
+        row = self.table.get(str(length))
+        ns = row["step_ns"] if row else float(length // 2 * max(1, (length // 2).bit_length() - 1))
+        return ns * self.sms * self.bps[length]
+
+    def item_lists(self):
+        """This tick's launches: per segment with busy slots, (segment, slots, steps), costliest
+        length first. Every item gets the steps that take as long as `quantum` steps of the
+        slowest busy length; when the busy slots need more blocks than the SMs hold at once (an
+        item of length L takes 1 / blocks_per_sm(L) of an SM), every budget shrinks by that
+        ratio, so a tick still lasts about one quantum of the slowest length."""
+        segs = [seg for segs in self.lanes.values() for seg in segs if seg.active]
+        if not segs:
+            return []
+        lat = {id(seg): self.item_lat_ns(seg) for seg in segs}
+        top = max(lat.values())
+        units = sum(len(seg.active) / self.bps[seg.batch.params.len] for seg in segs)
+        scale = min(1.0, self.sms / units)
+        jobs = []
+        for seg in sorted(segs, key=lambda sg: -lat[id(sg)]):
+            base = self.quantum * top / lat[id(seg)] * scale
+            slots, steps = [], []
+            for s in seg.active:
+                rem = seg.batch.remaining(s)
+                slots.append(s)
+                steps.append(max(1, min(rem, int(round(base)))))
+            order = sorted(range(len(slots)), key=lambda i: -steps[i])
+            jobs.append((seg, [slots[i] for i in order], [steps[i] for i in order]))
+        return jobs
+
     def tick(self) -> int:
         """One quantum on every busy slot, then the finished slots are read and freed."""
         t = time.perf_counter()
-        plan = self._plan()
-        items = self.work_list()
-        run = sum(it[2] for it in items)
-        t1 = time.perf_counter()
-        self.host_s["list"] += t1 - t
-        plan.run_items([it[0] for it in items], [it[1] for it in items], [it[2] for it in items])
+        if self.launch == "plan":
+            plan = self._plan()
+            items = self.work_list()
+            run = sum(it[2] for it in items)
+            t1 = time.perf_counter()
+            self.host_s["list"] += t1 - t
+            plan.run_items([it[0] for it in items], [it[1] for it in items], [it[2] for it in items])
+        else:
+            jobs = self.item_lists()
+            run = sum(sum(steps) for _, _, steps in jobs)
+            t1 = time.perf_counter()
+            self.host_s["list"] += t1 - t
+            for seg, slots, steps in jobs:
+                be, st = seg.batch.backend_and_state()
+                be.run_items_async(st, slots, steps)
+            if self.waiting:
+                # The launches run on the device; prepare waiting requests meanwhile (most of a
+                # tick's host work), leaving time to collect the results.
+                self.prepare(self.waiting, 0.8 * self.last_tick_s)
+            for seg, _, _ in jobs:
+                be, st = seg.batch.backend_and_state()
+                be.sync(st)
         t2 = time.perf_counter()
         self.gpu_s += t2 - t1
+        self.last_tick_s = t2 - t1
         now = t2 - self.t0
         self.steps_done += run
         self.ticks.append((now, self.busy(), run))
@@ -333,8 +420,12 @@ class Server:
 
     def serve(self, reqs):
         """Runs the whole stream in real time; returns the requests with their results."""
+        if self.launch == "stream":
+            return self.serve_stream(reqs)
         pending = deque(sorted(reqs, key=lambda r: r.arrival))
         waiting = deque()
+        self.waiting = waiting
+        self.last_tick_s = 0.0
         self.t0 = time.perf_counter()
         self.completed = 0
         while self.completed < len(reqs):
@@ -351,6 +442,86 @@ class Server:
                 time.sleep(max(0.0, min(0.05, pending[0].arrival - (time.perf_counter() - self.t0))))
             elif waiting and not self.busy():
                 raise MontMulError("a request fits no lane within the memory budget")
+        return reqs
+
+    def _collect(self, seg: Segment, now: float) -> int:
+        """After a segment's launch has finished: its errors, its finished slots read and freed."""
+        be, st = seg.batch.backend_and_state()
+        be.sync(st)
+        seg.inflight = False
+        done = [s for s in seg.active if seg.batch.remaining(s) == 0]
+        if not done:
+            return 0
+        raws = seg.batch.read_raw_slots(done)
+        for s, raw in zip(done, raws):
+            r = seg.active.pop(s)
+            m = seg.batch.moduli[s]
+            r.raw = raw
+            r.verdict = raw == m.r or raw == m.r + m.n
+            r.done = now
+            if self.checker is not None:
+                self.checker.submit(r)
+            seg.free.append(s)
+        return len(done)
+
+    def _launch(self, seg: Segment, slice_ns: float) -> int:
+        """One launch over the segment's busy slots, each budgeted about `slice_ns` of device time
+        (its length's time per step with the GPU full); returns the slot-steps enqueued."""
+        steps = max(1, int(slice_ns / self.item_lat_ns(seg)))
+        slots = sorted(seg.active, key=lambda s: -min(seg.batch.remaining(s), steps))
+        budget = [max(1, min(seg.batch.remaining(s), steps)) for s in slots]
+        be, st = seg.batch.backend_and_state()
+        be.run_items_async(st, slots, budget)
+        seg.inflight = True
+        return sum(budget)
+
+    def serve_stream(self, reqs):
+        """The stream without ticks: every segment runs its own cycle of launch, read, refill and
+        launch again on its own stream, at most one launch in flight per segment; the host
+        services whichever segment's launch has finished while the others keep the device busy,
+        and prepares waiting requests while it would otherwise wait."""
+        pending = deque(sorted(reqs, key=lambda r: r.arrival))
+        waiting = deque()
+        self.waiting = waiting
+        self.t0 = time.perf_counter()
+        self.completed = 0
+        slice_ns = self.slice_ms * 1e6
+        while self.completed < len(reqs):
+            now = time.perf_counter() - self.t0
+            while pending and pending[0].arrival <= now:
+                waiting.append(pending.popleft())
+            segs = [seg for segs in self.lanes.values() for seg in segs]
+            progressed = False
+            t = time.perf_counter()
+            for seg in segs:
+                if seg.inflight and not seg.batch.backend_and_state()[0].busy(seg.batch.backend_and_state()[1]):
+                    self.completed += self._collect(seg, time.perf_counter() - self.t0)
+                    progressed = True
+            t1 = time.perf_counter()
+            self.host_s["read"] += t1 - t
+            if waiting:
+                self.admit(waiting, now)
+                progressed = True
+            t2 = time.perf_counter()
+            self.host_s["admit"] += t2 - t1
+            for seg in [seg for segs in self.lanes.values() for seg in segs]:
+                if not seg.inflight and seg.active:
+                    run = self._launch(seg, slice_ns)
+                    self.steps_done += run
+                    self.ticks.append((time.perf_counter() - self.t0, self.busy(), run))
+                    progressed = True
+            self.host_s["list"] += time.perf_counter() - t2
+            if waiting:
+                self.prepare(waiting, 0.002)
+            if not progressed:
+                if not any(seg.inflight for segs in self.lanes.values() for seg in segs):
+                    if waiting:
+                        raise MontMulError("a request fits no lane within the memory budget")
+                    if pending:
+                        time.sleep(max(0.0, min(0.05, pending[0].arrival - (time.perf_counter() - self.t0))))
+                else:
+                    time.sleep(0.0002)
+        self.gpu_s = time.perf_counter() - self.t0 - sum(self.host_s.values())
         return reqs
 
     def close(self):
@@ -511,7 +682,7 @@ def summarize(server: Server, reqs, uniform_modsq: float, rate: float, cap: floa
         "steady_over_uniform": (win_modsq / uniform_modsq) if win_modsq else None,
         "p50_s": percentile(lat, 0.5), "p99_s": percentile(lat, 0.99),
         "mul_p50_s": percentile([r.done - r.arrival for r in muls], 0.5) if muls else None,
-        "ticks": len(server.ticks), "quantum": server.quantum,
+        "ticks": len(server.ticks), "quantum": server.quantum, "launch": server.launch, "slice_ms": server.slice_ms,
         "busy_slots_p50": percentile([b for t, b, _ in server.ticks if t_a <= t <= t_b], 0.5),
         "launch_time_frac": server.gpu_s / end,
         "host_time_frac": {k: v / end for k, v in server.host_s.items()},
@@ -540,20 +711,24 @@ def main(args) -> dict:
     ferm = [r for r in probe if r.kind == "fermat"]
     uniform = sum(r.n.bit_length() for r in ferm) / sum(
         r.n.bit_length() * step_s(Params.for_bits(r.n.bit_length(), lengths).len) for r in ferm)
-    results = []
+    results, pending = [], []
     for load in args.load:
         rate = load * cap
         count = max(8, int(round(rate * args.duration)))
         reqs = stream(count, rate, args.lo, args.hi, seed=args.seed)
+        # Each load's verdict checks keep running (in their own host threads) while the next
+        # load is served; they are all collected at the end.
         checker = None if args.no_check else VerdictChecker()
-        srv = Server(dev, quantum=args.quantum, checker=checker)
+        srv = Server(dev, quantum=args.quantum, checker=checker, launch=args.launch, slice_ms=args.slice_ms)
         with ClockSampler(args.device) as clk:
             srv.serve(reqs)
         srv.close()
         s = summarize(srv, reqs, uniform, rate, cap)
         s["clocks"] = clk.summary()
-        s["checked"] = check(dev, reqs, checker.finish()) if checker is not None else None
         results.append(s)
+        pending.append((s, reqs, checker))
+    for s, reqs, checker in pending:
+        s["checked"] = check(dev, reqs, checker.finish()) if checker is not None else None
     return {"workload": f"Poisson arrivals for {args.duration} s, bits log-uniform in [{args.lo}, {args.hi}], "
                         f"10% primes (seeded next_prime up to {PRIME_LIMIT_BITS} bits, Mersenne primes of about the "
                         f"drawn size above), 5% mul, full base-3 Fermat tests (seed {args.seed})",

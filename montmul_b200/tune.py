@@ -90,6 +90,13 @@ def fixed_parts(length: int, global_mode):
     return {"threads": threads_for(m), "blocks_per_sm": per_sm, "tile": None, "radix": radix_schedule(m)}
 
 
+def alt_threads(length: int) -> int:
+    """The alternative block shape of the shared-memory step at this length (mm_abi.h
+    alt_threads_for), 0 when none is built."""
+    m = (length // 2).bit_length() - 1
+    return {11: 256, 12: 256, 13: 1024}.get(m, 0)
+
+
 def candidates(length: int):
     n = length // 2
     modes = []
@@ -99,7 +106,11 @@ def candidates(length: int):
         modes.append(GLOBAL)
     if MIN_CLUSTER_N <= n <= MAX_CLUSTER_N:
         modes.append(CLUSTER)
-    return [(g, s) for g in modes for s in LAUNCH_STEPS]
+    out = []
+    for g in modes:
+        shapes = [0] + ([alt_threads(length)] if g == SHARED and alt_threads(length) else [])
+        out += [(g, s, th) for th in shapes for s in LAUNCH_STEPS]
+    return out
 
 
 def bits_for(length: int) -> int:
@@ -107,7 +118,8 @@ def bits_for(length: int) -> int:
     return 16 * length - 4
 
 
-def measure(dev, length: int, global_mode: bool, launch_steps: int, slots: int, steps: int, seed: int = 2026):
+def measure(dev, length: int, global_mode, launch_steps: int, slots: int, steps: int, seed: int = 2026,
+            threads: int = 0):
     """Seconds per slot-step of one schedule on a synthetic batch (random odd moduli at the top of
     the bucket, random exponents), after a warm-up launch."""
     from .batch import ModBatch
@@ -118,7 +130,7 @@ def measure(dev, length: int, global_mode: bool, launch_steps: int, slots: int, 
     exps = [rng.random_bits(steps + 8) | (1 << (steps + 7)) for _ in range(slots)]
     b = ModBatch(dev, moduli, 3)
     be, st = b.backend_and_state()
-    be.set_schedule(st, global_mode, launch_steps)
+    be.set_schedule(st, global_mode, launch_steps, 0.0, threads)
     b.load_all([1] * slots)
     b.set_exponents(exps)
     b.run(8)
@@ -162,15 +174,17 @@ def tune_length(dev, length: int, budget_s: float = 4.0):
     cands = candidates(length)
     steps = max(8, min(2000, int(budget_s / len(cands) / (probe * slots))))
     results = []
-    for g, s in cands:
-        sec = measure(dev, length, g, s, slots, steps)
-        results.append({"global": g, "launch_steps": s, "step_ns": sec * 1e9})
+    for g, s, th in cands:
+        sec = measure(dev, length, g, s, slots, steps, threads=th)
+        results.append({"global": g, "launch_steps": s, "block_threads": th, "step_ns": sec * 1e9})
     ranked = sorted(results, key=lambda r: r["step_ns"])
     best = ranked[0]
     out = dict(best)
     if len(ranked) > 1:
         out["runner_up"] = dict(ranked[1])
     out.update(fixed_parts(length, best["global"]))
+    if best.get("block_threads"):
+        out["threads"] = best["block_threads"]
     out["slots"] = slots
     out["steps"] = steps
     out["candidates"] = results
@@ -199,19 +213,29 @@ def save_table(table) -> None:
     os.replace(tmp, p)
 
 
-def schedule_for(device_name: str, length: int, table=None):
-    """The cached schedule of one length on one device, or None."""
+def schedule_for(device_name: str, length: int, table=None, cluster_ok: bool = True):
+    """The cached schedule of one length on one device, or None. Without `cluster_ok` (a batch
+    on the plain REDC path, which cluster mode does not run) a cluster-mode row gives way to its
+    fastest measured candidate in another mode."""
     table = load_table() if table is None else table
-    return table.get(device_name, {}).get(str(length))
+    row = table.get(device_name, {}).get(str(length))
+    if row and not cluster_ok and int(row["global"]) == CLUSTER:
+        others = [c for c in row.get("candidates", []) if int(c["global"]) != CLUSTER]
+        if not others:
+            return None
+        best = min(others, key=lambda c: c["step_ns"])
+        row = dict(row, **best)
+        row.pop("mixed_ns", None)
+    return row
 
 
 def apply(batch, table=None) -> bool:
     """Sets the cached schedule of the batch's length on its backend; False when none is cached."""
     be, st = batch.backend_and_state()
-    sc = schedule_for(be.device_name(), batch.params.len, table)
+    sc = schedule_for(be.device_name(), batch.params.len, table, getattr(be, "wraparound", True))
     if not sc:
         return False
-    be.set_schedule(st, sc["global"], sc["launch_steps"], sc.get("mixed_ns", sc["step_ns"]))
+    be.set_schedule(st, sc["global"], sc["launch_steps"], sc.get("mixed_ns", sc["step_ns"]), sc.get("block_threads", 0))
     return True
 
 

@@ -134,3 +134,39 @@ def test_two_batches_interleaved(gpu):
     for b, moduli, exps in batches:
         for i in range(4):
             assert b.read(i) == powm(3, exps[i], moduli[i])
+
+
+@pytest.mark.parametrize("length,alt", [(4096, 256), (8192, 256), (16384, 1024)])
+def test_alternative_block_shape_same_raw(gpu, wrap, length, alt):
+    """The alternative block shape a schedule may select (threads per block, mm_abi.h
+    alt_threads_for) runs the same steps: raw limbs equal the oracle's, and switching shapes in
+    the middle of a run changes nothing."""
+    dev = gpu()
+
+    class Alt:
+        def __getattr__(self, name):
+            return getattr(dev, name)
+
+        def create(self, *a):
+            st = dev.create(*a)
+            dev.set_schedule(st, 0, 5, 0.0, alt)
+            assert dev.get_schedule(st)["threads"] == alt
+            return st
+
+    common.same_raw(lambda: Alt(), wrap, 16 * length - 4, 3, 12)
+    rng = RandState(length)
+    moduli = [common.rand_odd(rng, 16 * length - 4) for _ in range(4)]
+    exps = [common.rand_exponent(rng, 20) for _ in range(4)]
+    a, b = ModBatch(dev, moduli, 3), ModBatch(dev, moduli, 3)
+    for x in (a, b):
+        x.load_all([1] * 4)
+        x.set_exponents(exps)
+    be, st = a.backend_and_state()
+    be.set_schedule(st, 0, 0, 0.0, alt)
+    a.run(7)
+    be.set_schedule(st, 0, 0, 0.0, 0)
+    a.run(20)
+    b.run(20)
+    assert [a.read_raw(i) for i in range(4)] == [b.read_raw(i) for i in range(4)]
+    with pytest.raises(MontMulError, match="threads per block"):
+        be.set_schedule(st, 0, 0, 0.0, 96)

@@ -61,6 +61,32 @@ def test_mixed_plan_same_as_alone(dev, quantum):
     plan.close()
 
 
+@pytest.mark.parametrize("quantum", [9, 1 << 16])
+def test_mixed_plan_cluster_items(dev, quantum):
+    """L = 32768 batches in cluster mode run as cluster items of the mixed launch (a block pair on
+    one slot), beside an L = 32768 batch in global mode on the workers and shorter lengths; every
+    slot ends as it does alone, and with pow_mod."""
+    from montmul_b200.backend import Plan
+    spec = _batches(dev, [300_000, 400_000, 500_000, 100_000, 250_000], 4, 33, 23)
+    mixed = _arm(dev, spec)
+    modes = [2, 1, 2, 1, 0]
+    for b, mode in zip(mixed, modes):
+        be, st = b.backend_and_state()
+        be.set_schedule(st, mode, 0)
+    assert [b.params.len for b in mixed] == [32768, 32768, 32768, 8192, 16384]
+    plan = Plan(mixed, quantum)
+    plan.run(33)
+    alone = _arm(dev, spec)
+    for b in alone:
+        b.run(33)
+    for (moduli, exps, base), bm, ba in zip(spec, mixed, alone):
+        for i in range(len(moduli)):
+            assert bm.remaining(i) == 0
+            assert bm.read_raw(i) == ba.read_raw(i), f"L {bm.params.len} slot {i}"
+        assert bm.read(0) == powm(base, exps[0], moduli[0])
+    plan.close()
+
+
 def test_mixed_plan_partial_runs(dev):
     """plan.run(bits) advances every slot by at most `bits`; uneven exponent lengths finish at
     their own step."""

@@ -24,7 +24,10 @@ def _alone_raw(dev, n):
     return b.read_raw(0)
 
 
-def test_served_stream_same_as_alone(dev):
+@pytest.mark.parametrize("launch", ["stream", "items", "plan"])
+def test_served_stream_same_as_alone(dev, launch):
+    """Every launch mode: segments that launch, read and refill on their own streams; ticks of
+    per-segment uniform launches over slot lists; ticks of one mixed-length persistent plan."""
     from montmul_b200 import serve
     # Seeded next_prime primes up to 6,000 bits (a quick search), Mersenne primes above.
     reqs = serve.stream(40, 400.0, 2000, 40_000, prime_frac=0.2, mul_frac=0.1, seed=20, prime_limit=6000)
@@ -32,7 +35,7 @@ def test_served_stream_same_as_alone(dev):
     # Small segments force several segments per lane and waiting requests; every verdict is
     # checked while the stream runs.
     checker = serve.VerdictChecker(threads=4)
-    srv = serve.Server(dev, quantum=64, segment_slots=6, tuned=False, checker=checker)
+    srv = serve.Server(dev, quantum=64, segment_slots=6, tuned=False, checker=checker, launch=launch, slice_ms=2.0)
     srv.serve(reqs)
     srv.close()
     assert all(r.done is not None for r in reqs)
@@ -53,6 +56,29 @@ def test_served_stream_same_as_alone(dev):
     assert c["verdicts"] == len(ferm) == c["mersenne_prime"] + c["small_factor"] + c["gmp_powm"]
     assert c["mersenne_prime"] == sum(1 for r in ferm if r.prime == "mersenne")
     assert c["alone"] == 5
+
+
+def test_run_items_steps_listed_slots_only(dev):
+    """mm_b200_run_items_async: listed slots advance by their own budgets (capped at what they have
+    left), unlisted ones stay; the results are those of plain run()."""
+    from montmul_b200.gmp import RandState
+    rng = RandState(9)
+    moduli = [rng.random_bits(30_000) | (1 << 29_999) | 1 for _ in range(6)]
+    exps = [rng.random_bits(40) | (1 << 39) for _ in range(6)]
+    a, b = ModBatch(dev, moduli, 3), ModBatch(dev, moduli, 3)
+    for x in (a, b):
+        x.load_all([1] * 6)
+        x.set_exponents(exps)
+    be, st = a.backend_and_state()
+    be.run_items_async(st, [4, 1, 2], [10, 3, 100])
+    be.sync(st)
+    assert [a.remaining(i) for i in range(6)] == [40, 37, 0, 40, 30, 40]
+    be.run_items_async(st, [0, 1, 3, 4, 5], [40, 37, 40, 30, 40])
+    be.sync(st)
+    b.run(40)
+    assert [a.read_raw(i) for i in range(6)] == [b.read_raw(i) for i in range(6)]
+    for i in range(6):
+        assert a.read(i) == powm(3, exps[i], moduli[i])
 
 
 def test_fermat_driver_on_mersenne_primes(dev):

@@ -23,12 +23,13 @@ def test_radix_schedule_covers_every_stage():
 
 def test_tune_candidates_by_length():
     S, G, C = tune.SHARED, tune.GLOBAL, tune.CLUSTER
-    assert tune.candidates(4096) == [(S, s) for s in tune.LAUNCH_STEPS]
-    assert {g for g, _ in tune.candidates(8192)} == {S, G}
-    assert {g for g, _ in tune.candidates(16384)} == {S, G}
-    assert {g for g, _ in tune.candidates(32768)} == {G, C}
-    assert {g for g, _ in tune.candidates(65536)} == {G, C}
-    assert {g for g, _ in tune.candidates(131072)} == {G}
+    assert tune.candidates(2048) == [(S, s, 0) for s in tune.LAUNCH_STEPS]
+    assert {(c[0], c[2]) for c in tune.candidates(4096)} == {(S, 0), (S, 256)}
+    assert {(c[0], c[2]) for c in tune.candidates(8192)} == {(S, 0), (S, 256), (G, 0)}
+    assert {(c[0], c[2]) for c in tune.candidates(16384)} == {(S, 0), (S, 1024), (G, 0)}
+    assert {c[0] for c in tune.candidates(32768)} == {G, C}
+    assert {c[0] for c in tune.candidates(65536)} == {G, C}
+    assert {c[0] for c in tune.candidates(131072)} == {G}
     assert tune.fixed_parts(1 << 20, True)["radix"]["global"] == tune.radix_schedule(19 - 11)
     assert tune.fixed_parts(32768, C)["cluster"] == 2 and tune.fixed_parts(65536, C)["cluster"] == 4
     assert [tune.mode_name(m) for m in (S, G, C, False, True)] == ["shared", "global", "cluster", "shared", "global"]
@@ -40,6 +41,24 @@ def test_tune_table_roundtrip(tmp_path, monkeypatch):
     assert tune.schedule_for("dev", 8192)["step_ns"] == 680.0
     assert tune.schedule_for("dev", 4096) is None
     assert tune.schedule_for("other", 8192) is None
+
+
+def test_cluster_row_gives_way_on_the_plain_path(tmp_path, monkeypatch):
+    """A batch on the plain REDC path (no wraparound) cannot run cluster mode: it takes the
+    fastest measured candidate of another mode from the same row."""
+    monkeypatch.setenv("MONTMUL_B200_SCHEDULES", str(tmp_path / "s.json"))
+    cands = [{"global": 1, "launch_steps": 64, "step_ns": 4903.0, "block_threads": 0},
+             {"global": 1, "launch_steps": 512, "step_ns": 5211.0, "block_threads": 0},
+             {"global": 2, "launch_steps": 512, "step_ns": 4118.0, "block_threads": 0}]
+    tune.save_table({"dev": {"32768": {"global": 2, "launch_steps": 512, "step_ns": 4118.0, "cluster": 2,
+                                       "mixed_ns": 4385.0, "candidates": cands},
+                             "65536": {"global": 2, "launch_steps": 512, "step_ns": 10293.0,
+                                       "candidates": cands[2:]}}})
+    assert tune.schedule_for("dev", 32768)["global"] == 2
+    row = tune.schedule_for("dev", 32768, cluster_ok=False)
+    assert (row["global"], row["launch_steps"], row["step_ns"]) == (1, 64, 4903.0) and "mixed_ns" not in row
+    assert tune.schedule_for("dev", 65536, cluster_ok=False) is None
+    assert tune.load_table()["dev"]["32768"]["global"] == 2   # the table itself is unchanged
 
 
 class _FakeDev:
@@ -87,6 +106,30 @@ def test_mixed_workload():
     below = sum(1 for bits, *_ in w if bits < mid)
     assert 200 < below < 300
     assert {Params.for_bits(b, LENGTHS).len for b, *_ in w} == {1024, 2048, 4096, 8192, 16384, 32768}
+
+
+def test_admission_waits_for_an_inflight_segment_with_room():
+    """A segment whose launch is on the device takes no refill; a request of its length waits
+    for it while it has room, and the lane grows only when no segment has room."""
+    srv = object.__new__(serve.Server)
+    grown = []
+
+    def grow(length):
+        seg = serve.Segment(batch=None, free=[0, 1])
+        srv.lanes.setdefault(length, []).append(seg)
+        grown.append(length)
+        return seg
+
+    srv._grow = grow
+    busy = serve.Segment(batch=None, free=[5, 6], inflight=True)
+    srv.lanes = {8192: [busy]}
+    assert srv._slots_for(8192, 1) == (None, None) and not grown
+    busy.inflight = False
+    seg, slots = srv._slots_for(8192, 2)
+    assert seg is busy and slots == [6, 5] and not grown
+    busy.inflight = True   # full and in flight: the lane grows
+    seg, slots = srv._slots_for(8192, 1)
+    assert grown == [8192] and seg is srv.lanes[8192][1] and slots == [1]
 
 
 def test_serve_stream():
