@@ -104,8 +104,8 @@ __device__ __noinline__ uint64_t carry_product(const F2* s2, const F1* s1, uint3
         Acc96 acc;
 #pragma unroll
         for (int e = 0; e < E; ++e) {
-            const F2 a2 = s2[swz(j0 + e)];
-            const F1 a1 = s1[swz(j0 + e)];
+            const F2 a2 = s2[(swz(j0) ^ swz_c(e))];
+            const F1 a1 = s1[(swz(j0) ^ swz_c(e))];
             uint32_t w0, w1, w2;
             crt3(hi ? a1.im : a1.re, hi ? a2.im : a2.re, w0, w1, w2);
             L[e] = acc.add_shift(w0, w1, w2);
@@ -139,7 +139,7 @@ __device__ __noinline__ void carry_low_and_pack(F2* s2, F1* s1, uint64_t* sc) {
 #pragma unroll
         for (int e = 0; e < E; ++e) {
             uint32_t w0, w1, w2;
-            crt3(s1[swz(q0 + e)].re, s2[swz(q0 + e)].re, w0, w1, w2);
+            crt3(s1[(swz(q0) ^ swz_c(e))].re, s2[(swz(q0) ^ swz_c(e))].re, w0, w1, w2);
             L[e] = acc.add_shift(w0, w1, w2);
         }
         c = acc.rest();
@@ -151,12 +151,13 @@ __device__ __noinline__ void carry_low_and_pack(F2* s2, F1* s1, uint64_t* sc) {
     if (t < TA) {
 #pragma unroll
         for (int e = 0; e < E; e += 2) {
-            const int j = (q0 + e) >> 1;
+            // (q0 + e) / 2, q0 / 2 a multiple of E / 2: swz of the sum is the XOR of the parts
+            const int sj = swz(q0 >> 1) ^ swz_c(e >> 1);
             F2 z2; z2.re = L[e]; z2.im = L[e + 1];
             uint32_t r0 = (L[e] & P1) + (L[e] >> 31), r1 = (L[e + 1] & P1) + (L[e + 1] >> 31);
             F1 z1; z1.re = min(r0, r0 - P1); z1.im = min(r1, r1 - P1);
-            s2[swz(j)] = z2;
-            s1[swz(j)] = z1;
+            s2[sj] = z2;
+            s1[sj] = z1;
         }
     }
     gsync<NT>();
@@ -178,7 +179,7 @@ __device__ __noinline__ void carry_low_to(const F2* s2, const F1* s1, uint32_t* 
 #pragma unroll
         for (int e = 0; e < E; ++e) {
             uint32_t w0, w1, w2;
-            crt3(s1[swz(q0 + e)].re, s2[swz(q0 + e)].re, w0, w1, w2);
+            crt3(s1[(swz(q0) ^ swz_c(e))].re, s2[(swz(q0) ^ swz_c(e))].re, w0, w1, w2);
             L[e] = acc.add_shift(w0, w1, w2);
         }
         c = acc.rest();
@@ -215,8 +216,8 @@ __device__ __noinline__ bool carry_shift_add(const F2* s2, const F1* s1, const u
 #pragma unroll
         for (int e = 0; e < E; ++e) {
             const int q = q0 + e;
-            const F2 a2 = s2[swz(j0 + e)];
-            const F1 a1 = s1[swz(j0 + e)];
+            const F2 a2 = s2[(swz(j0) ^ swz_c(e))];
+            const F1 a1 = s1[(swz(j0) ^ swz_c(e))];
             uint32_t w0, w1, w2;
             crt3(hi ? a1.im : a1.re, hi ? a2.im : a2.re, w0, w1, w2);
             const uint64_t add = (q >= k && q < 2 * k ? (uint64_t)tl[q] : 0u) + (q == k ? flag : 0u);
@@ -259,9 +260,10 @@ __device__ __noinline__ bool wrap_combine(const F2* s2, const F1* s1, const uint
         Acc96 acc;
 #pragma unroll
         for (int e = 0; e < E; e += 2) {
-            const int j = (q0 + e) >> 1;
-            const F2 a2 = s2[swz(j)];
-            const F1 a1 = s1[swz(j)];
+            // (q0 + e) / 2, q0 / 2 a multiple of E / 2: swz of the sum is the XOR of the parts
+            const int sj = swz(q0 >> 1) ^ swz_c(e >> 1);
+            const F2 a2 = s2[sj];
+            const F1 a1 = s1[sj];
             uint32_t w0, w1, w2;
             crt3(a1.re, a2.re, w0, w1, w2);
             uint64_t lo = (((uint64_t)w1 << 32) | w0) + tl[q0 + e];

@@ -10,8 +10,15 @@
 // position ends with exactly the value the reference's radix-2 loops produce.
 //
 // Shared-memory layout: F2 array (16 B per element) then F1 array (8 B), element e stored at
-// swz(e). swz flips the low 3 bits by bits 3-5 and bit 3 by bit 6, which makes every radix-8 and
-// radix-4 pass free of bank conflicts in both arrays (checked by simulation over all spans).
+// swz(e): e with its low four bits flipped by a linear function of bits 3-8,
+//   bit 0 ^= e3 ^ e6 ^ e8,  bit 1 ^= e4 ^ e6 ^ e7,  bit 2 ^= e5,  bit 3 ^= e4 ^ e5 ^ e6.
+// Simulated over every shared-memory access pattern of the kernels (each radix-8 and radix-4 pass
+// of both transforms at every span; the carries' runs of 2 to 32 consecutive elements per
+// thread and their pair-packed reads and writes; 16-B F2 and 8-B F1 accesses; 32 to 1,024
+// threads per slot), every warp access of n >= 64 elements takes the minimum number of
+// wavefronts. (Flipping the low bits by bits 3-6 alone left the carries' runs of 16 and 32
+// elements 2- and 4-way conflicted.) swz is linear over XOR, swz(a ^ b) = swz(a) ^ swz(b), and
+// permutes each aligned run of 16 elements.
 #pragma once
 #include "mm_field.cuh"
 
@@ -42,12 +49,13 @@ template <int NT> __device__ __forceinline__ int gsync_or(int pred) {
     return r;
 }
 
-__device__ __forceinline__ int swz(int e) {
-    return (e & ~15) | ((((e >> 3) ^ (e >> 6)) & 1) << 3) | ((e ^ (e >> 3)) & 7);
-}
 MM_HD constexpr int swz_c(int e) {
-    return (e & ~15) | ((((e >> 3) ^ (e >> 6)) & 1) << 3) | ((e ^ (e >> 3)) & 7);
+    const int h = e >> 3, u = (h >> 3) & 7;   // h: bits 3.., u: bits 6-8
+    const int lo = (h ^ ((u ^ (u << 1) ^ (u >> 2)) & 3)) & 7;
+    const int b3 = ((h >> 1) ^ (h >> 2) ^ (h >> 3)) & 1;
+    return e ^ lo ^ (b3 << 3);
 }
+__device__ __forceinline__ int swz(int e) { return swz_c(e); }
 
 // ---- in-register butterflies (positions k of one group) ----
 // u + (-i) v and u - (-i) v
@@ -174,18 +182,19 @@ template <> __device__ __forceinline__ void bf_dit<8, F2>(F2* x) { bf_dit8(x); }
 template <int R, bool FWD, int NT, bool TW>
 __device__ __noinline__ void pass_rt(F2* s2, F1* s1, const F2K* __restrict__ t2, const F1* __restrict__ t1, int LQ, int G) {
     const int q = 1 << LQ;
-    int ko[R];   // swz(k q): the span is a runtime value, so the k offsets are formed once per pass
-#pragma unroll
-    for (int k = 0; k < R; ++k) ko[k] = swz(k * q);
+    // swz(k q) for k < R: swz is linear over XOR, so the offsets are XORs of those of the
+    // span's powers of two q, 2q, 4q (three registers instead of R).
+    const int kb0 = swz(q), kb1 = R > 2 ? swz(2 * q) : 0, kb2 = R > 4 ? swz(4 * q) : 0;
+#define MM_KO(k) ((((k) & 1) ? kb0 : 0) ^ (((k) & 2) ? kb1 : 0) ^ (((k) & 4) ? kb2 : 0))
 #pragma unroll 1
     for (int g = gtid<NT>(); g < G; g += NT) {
         const int j = g & (q - 1);
-        // b + k q has disjoint bits, and swz is linear over XOR: swz(b + k q) = swz(b) ^ swz(k q).
+        // b + k q has disjoint bits: swz(b + k q) = swz(b) ^ swz(k q).
         const int sb = swz(((g >> LQ) << (LQ + ilog2c(R))) + j);
         {
             F2 x[R];
 #pragma unroll
-            for (int k = 0; k < R; ++k) x[k] = s2[sb ^ ko[k]];
+            for (int k = 0; k < R; ++k) x[k] = s2[sb ^ MM_KO(k)];
             if (FWD) {
                 ldif<R>(x);
                 x[0] = lcfold(x[0]);
@@ -199,12 +208,12 @@ __device__ __noinline__ void pass_rt(F2* s2, F1* s1, const F2K* __restrict__ t2,
                 ldit<R>(x);
             }
 #pragma unroll
-            for (int k = 0; k < R; ++k) s2[sb ^ ko[k]] = x[k];
+            for (int k = 0; k < R; ++k) s2[sb ^ MM_KO(k)] = x[k];
         }
         {
             F1 x[R];
 #pragma unroll
-            for (int k = 0; k < R; ++k) x[k] = s1[sb ^ ko[k]];
+            for (int k = 0; k < R; ++k) x[k] = s1[sb ^ MM_KO(k)];
             if (FWD) {
                 bf_dif<R, F1>(x);
                 if (TW) {
@@ -219,9 +228,10 @@ __device__ __noinline__ void pass_rt(F2* s2, F1* s1, const F2K* __restrict__ t2,
                 bf_dit<R, F1>(x);
             }
 #pragma unroll
-            for (int k = 0; k < R; ++k) s1[sb ^ ko[k]] = x[k];
+            for (int k = 0; k < R; ++k) s1[sb ^ MM_KO(k)] = x[k];
         }
     }
+#undef MM_KO
     gsync<NT>();
 }
 
@@ -252,6 +262,7 @@ __device__ __noinline__ void dif_first_from_limbs(const uint32_t* __restrict__ l
     constexpr int toff = tab_fwd_off(M, 0, true), coff = tab_in_const_off(M, true);
 #pragma unroll 1
     for (int j = gtid<NT>(); j < Q; j += NT) {
+        const int sj = swz(j);   // j < Q: swz(j + k Q) = swz(j) ^ swz(k Q)
         uint32_t v[R];
 #pragma unroll
         for (int k = 0; k < R; ++k) v[k] = (j + k * Q < cnt) ? lim[j + k * Q] : 0u;
@@ -261,7 +272,7 @@ __device__ __noinline__ void dif_first_from_limbs(const uint32_t* __restrict__ l
             for (int k = 0; k < R; ++k) x[k] = lreal_times(v[k], tab2[coff + k]);
             ldif<R>(x);
 #pragma unroll
-            for (int k = 0; k < R; ++k) s2[swz(j + k * Q)] = lkmul(lcfold(x[k]), tab2[toff + k * Q + j]);
+            for (int k = 0; k < R; ++k) s2[(sj ^ swz_c(k * Q))] = lkmul(lcfold(x[k]), tab2[toff + k * Q + j]);
         }
         {
             F1 x[R];
@@ -269,7 +280,7 @@ __device__ __noinline__ void dif_first_from_limbs(const uint32_t* __restrict__ l
             for (int k = 0; k < R; ++k) x[k] = real_times<F1>(v[k], tab1[coff + k]);
             bf_dif<R, F1>(x);
 #pragma unroll
-            for (int k = 0; k < R; ++k) s1[swz(j + k * Q)] = cmul(x[k], tab1[toff + k * Q + j]);
+            for (int k = 0; k < R; ++k) s1[(sj ^ swz_c(k * Q))] = cmul(x[k], tab1[toff + k * Q + j]);
         }
     }
     gsync<NT>();
@@ -284,26 +295,27 @@ __device__ __noinline__ void dit_last_weighted(F2* s2, F1* s1, const F2K* tab2, 
     constexpr int toff = tab_inv_off(M, 0, true), coff = tab_out_const_off(M, true);
 #pragma unroll 1
     for (int j = gtid<NT>(); j < Q; j += NT) {
+        const int sj = swz(j);   // j < Q: swz(j + k Q) = swz(j) ^ swz(k Q)
         {
             F2 x[R];
 #pragma unroll
-            for (int k = 0; k < R; ++k) x[k] = lkmul(s2[swz(j + k * Q)], tab2[toff + k * Q + j]);
+            for (int k = 0; k < R; ++k) x[k] = lkmul(s2[(sj ^ swz_c(k * Q))], tab2[toff + k * Q + j]);
             ldit<R>(x);
 #pragma unroll
             for (int k = 0; k < R; ++k) {
-                if (REAL_ONLY) s2[swz(j + k * Q)].re = lkmul_re(x[k], tab2[coff + k]);
-                else s2[swz(j + k * Q)] = lkmul(x[k], tab2[coff + k]);
+                if (REAL_ONLY) s2[(sj ^ swz_c(k * Q))].re = lkmul_re(x[k], tab2[coff + k]);
+                else s2[(sj ^ swz_c(k * Q))] = lkmul(x[k], tab2[coff + k]);
             }
         }
         {
             F1 x[R];
 #pragma unroll
-            for (int k = 0; k < R; ++k) x[k] = cmul(s1[swz(j + k * Q)], tab1[toff + k * Q + j]);
+            for (int k = 0; k < R; ++k) x[k] = cmul(s1[(sj ^ swz_c(k * Q))], tab1[toff + k * Q + j]);
             bf_dit<R, F1>(x);
 #pragma unroll
             for (int k = 0; k < R; ++k) {
-                if (REAL_ONLY) s1[swz(j + k * Q)].re = cmul_re(x[k], tab1[coff + k]);
-                else s1[swz(j + k * Q)] = cmul(x[k], tab1[coff + k]);
+                if (REAL_ONLY) s1[(sj ^ swz_c(k * Q))].re = cmul_re(x[k], tab1[coff + k]);
+                else s1[(sj ^ swz_c(k * Q))] = cmul(x[k], tab1[coff + k]);
             }
         }
     }
@@ -320,22 +332,23 @@ __device__ __noinline__ void dif_first_complex(F2* s2, F1* s1, const F2K* tab2, 
     constexpr int toff = tab_fwd_off(M, 0, true), coff = tab_in_const_off(M, true);
 #pragma unroll 1
     for (int j = gtid<NT>(); j < Q; j += NT) {
+        const int sj = swz(j);   // j < Q: swz(j + k Q) = swz(j) ^ swz(k Q)
         {
             F2 x[R];
 #pragma unroll
-            for (int k = 0; k < R; ++k) x[k] = lkmul(s2[swz(j + k * Q)], tab2[coff + k]);
+            for (int k = 0; k < R; ++k) x[k] = lkmul(s2[(sj ^ swz_c(k * Q))], tab2[coff + k]);
             ldif<R>(x);
 #pragma unroll
             for (int k = 0; k < R; ++k)
-                s2[swz(j + k * Q)] = Q > 1 ? lkmul(lcfold(x[k]), tab2[toff + k * Q + j]) : lcfold(x[k]);
+                s2[(sj ^ swz_c(k * Q))] = Q > 1 ? lkmul(lcfold(x[k]), tab2[toff + k * Q + j]) : lcfold(x[k]);
         }
         {
             F1 x[R];
 #pragma unroll
-            for (int k = 0; k < R; ++k) x[k] = cmul(s1[swz(j + k * Q)], tab1[coff + k]);
+            for (int k = 0; k < R; ++k) x[k] = cmul(s1[(sj ^ swz_c(k * Q))], tab1[coff + k]);
             bf_dif<R, F1>(x);
 #pragma unroll
-            for (int k = 0; k < R; ++k) s1[swz(j + k * Q)] = Q > 1 ? cmul(x[k], tab1[toff + k * Q + j]) : x[k];
+            for (int k = 0; k < R; ++k) s1[(sj ^ swz_c(k * Q))] = Q > 1 ? cmul(x[k], tab1[toff + k * Q + j]) : x[k];
         }
     }
     gsync<NT>();
@@ -348,22 +361,23 @@ __device__ __noinline__ void dit_last_complex(F2* s2, F1* s1, const F2K* tab2, c
     constexpr int toff = tab_inv_off(M, 0, true), coff = tab_out_const_off(M, true);
 #pragma unroll 1
     for (int j = gtid<NT>(); j < Q; j += NT) {
+        const int sj = swz(j);   // j < Q: swz(j + k Q) = swz(j) ^ swz(k Q)
         {
             F2 x[R];
 #pragma unroll
             for (int k = 0; k < R; ++k)
-                x[k] = Q > 1 ? lkmul(s2[swz(j + k * Q)], tab2[toff + k * Q + j]) : s2[swz(j + k * Q)];
+                x[k] = Q > 1 ? lkmul(s2[(sj ^ swz_c(k * Q))], tab2[toff + k * Q + j]) : s2[(sj ^ swz_c(k * Q))];
             ldit<R>(x);
 #pragma unroll
-            for (int k = 0; k < R; ++k) s2[swz(j + k * Q)] = lkmul(x[k], tab2[coff + k]);
+            for (int k = 0; k < R; ++k) s2[(sj ^ swz_c(k * Q))] = lkmul(x[k], tab2[coff + k]);
         }
         {
             F1 x[R];
 #pragma unroll
-            for (int k = 0; k < R; ++k) x[k] = Q > 1 ? cmul(s1[swz(j + k * Q)], tab1[toff + k * Q + j]) : s1[swz(j + k * Q)];
+            for (int k = 0; k < R; ++k) x[k] = Q > 1 ? cmul(s1[(sj ^ swz_c(k * Q))], tab1[toff + k * Q + j]) : s1[(sj ^ swz_c(k * Q))];
             bf_dit<R, F1>(x);
 #pragma unroll
-            for (int k = 0; k < R; ++k) s1[swz(j + k * Q)] = cmul(x[k], tab1[coff + k]);
+            for (int k = 0; k < R; ++k) s1[(sj ^ swz_c(k * Q))] = cmul(x[k], tab1[coff + k]);
         }
     }
     gsync<NT>();
@@ -382,6 +396,7 @@ __device__ __noinline__ void fused_mid(const uint32_t* __restrict__ lim, int cnt
     constexpr int cin = tab_in_const_off(M, true), cout = tab_out_const_off(M, true);
 #pragma unroll 1
     for (int g = gtid<NT>(); g < G; g += NT) {
+        const int sg = swz(R * g);   // swz(R g + k) = swz(R g) ^ k for k < R <= 8
         {
             F2 x[R];
             if (single) {
@@ -389,7 +404,7 @@ __device__ __noinline__ void fused_mid(const uint32_t* __restrict__ lim, int cnt
                 for (int k = 0; k < R; ++k) x[k] = lreal_times(k < cnt ? lim[k] : 0u, tab2[cin + k]);
             } else {
 #pragma unroll
-                for (int k = 0; k < R; ++k) x[k] = s2[swz(R * g + k)];
+                for (int k = 0; k < R; ++k) x[k] = s2[(sg ^ k)];
             }
             ldif<R>(x);
 #pragma unroll
@@ -402,7 +417,7 @@ __device__ __noinline__ void fused_mid(const uint32_t* __restrict__ lim, int cnt
                         if (REAL_ONLY) s2[k].re = lkmul_re(x[k], tab2[cout + k]);
                         else s2[k] = lkmul(x[k], tab2[cout + k]);
                     } else {
-                        s2[swz(R * g + k)] = x[k];
+                        s2[(sg ^ k)] = x[k];
                     }
                 }
             }
@@ -414,7 +429,7 @@ __device__ __noinline__ void fused_mid(const uint32_t* __restrict__ lim, int cnt
                 for (int k = 0; k < R; ++k) x[k] = real_times<F1>(k < cnt ? lim[k] : 0u, tab1[cin + k]);
             } else {
 #pragma unroll
-                for (int k = 0; k < R; ++k) x[k] = s1[swz(R * g + k)];
+                for (int k = 0; k < R; ++k) x[k] = s1[(sg ^ k)];
             }
             bf_dif<R, F1>(x);
             if (!op.template apply1<R>(x, g)) {
@@ -425,7 +440,7 @@ __device__ __noinline__ void fused_mid(const uint32_t* __restrict__ lim, int cnt
                         if (REAL_ONLY) s1[k].re = cmul_re(x[k], tab1[cout + k]);
                         else s1[k] = cmul(x[k], tab1[cout + k]);
                     } else {
-                        s1[swz(R * g + k)] = x[k];
+                        s1[(sg ^ k)] = x[k];
                     }
                 }
             }

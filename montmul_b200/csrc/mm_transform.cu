@@ -42,7 +42,7 @@ namespace {
         if (e_ != cudaSuccess) return mm_set_error(MM_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
     } while (0)
 
-int swz_host(int e) { return (e & ~15) | ((((e >> 3) ^ (e >> 6)) & 1) << 3) | ((e ^ (e >> 3)) & 7); }
+int swz_host(int e) { return swz_c(e); }
 
 int log2_len(size_t len) {
     int l = 0;
