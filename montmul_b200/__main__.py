@@ -255,7 +255,7 @@ def main(argv=None) -> int:
     p.add_argument("--launch", choices=["stream", "items", "plan"], default="stream",
                    help="stream: every segment launches, reads and refills on its own; items: ticks of "
                         "per-segment launches; plan: ticks of one mixed-length launch")
-    p.add_argument("--slice-ms", type=float, default=30.0, help="stream: device time budgeted per launch")
+    p.add_argument("--slice-ms", type=float, default=120.0, help="stream: device time budgeted per launch")
     p = sub.add_parser("tune", allow_abbrev=False)
     p.add_argument("--lengths", type=int, nargs="*", default=[1 << e for e in range(8, 18)])
     p.add_argument("--force", action="store_true")

@@ -37,6 +37,21 @@ template <int C> struct Chunks {
     template <int LOG> __device__ __forceinline__ F1& e1(int e) const { return c1[e >> LOG][swz(e & ((1 << LOG) - 1))]; }
 };
 
+// Element j + k Q of a vector spread in chunks of 2^LOG elements, for j < Q where Q divides the
+// chunk length: its chunk, (k Q) >> LOG, and its position's swz offset, swz((k Q) mod 2^LOG), are
+// fixed by k, so an unrolled loop over k addresses it with the chunk pointers in registers and
+// swz(j) ^ a constant (swz is linear over XOR, and j and (k Q) mod 2^LOG have disjoint bits).
+template <int LOG, int Q> __device__ __forceinline__ constexpr int kchunk(int k) { return (k * Q) >> LOG; }
+template <int LOG, int Q> __device__ __forceinline__ constexpr int koff(int k) { return swz_c((k * Q) & ((1 << LOG) - 1)); }
+template <int C> struct ChunkRegs {
+    F2* c2[C];
+    F1* c1[C];
+    __device__ __forceinline__ explicit ChunkRegs(const Chunks<C>& ch) {
+#pragma unroll
+        for (int d = 0; d < C; ++d) { c2[d] = ch.c2[d]; c1[d] = ch.c1[d]; }
+    }
+};
+
 // Per-CTA scratch of the cluster carry (each CTA's own copy; peers write into it).
 struct ClusterCarry {
     uint64_t cin_prev;   // segment carry of the previous CTA's last thread
@@ -129,8 +144,11 @@ __device__ __noinline__ void cl_dif_first(const uint32_t* __restrict__ lim, int 
     // reads the chunks this pass overwrites.
     cl.sync();
     const int j0 = (int)cl.block_rank() * QC;
+    const ChunkRegs<C> cr(ch);
+    static_assert((1 << kChunkLog) % Q == 0, "the passes' spans divide the chunk length");
 #pragma unroll 1
     for (int j = j0 + (int)threadIdx.x; j < j0 + QC; j += NT) {
+        const int sj = swz(j);
         uint32_t v[R];
 #pragma unroll
         for (int k = 0; k < R; ++k) v[k] = (j + k * Q < cnt) ? lim[j + k * Q] : 0u;
@@ -140,7 +158,7 @@ __device__ __noinline__ void cl_dif_first(const uint32_t* __restrict__ lim, int 
             for (int k = 0; k < R; ++k) x[k] = lreal_times(v[k], tab2[coff + k]);
             ldif<R>(x);
 #pragma unroll
-            for (int k = 0; k < R; ++k) ch.template e2<kChunkLog>(j + k * Q) = lkmul(lcfold(x[k]), tab2[toff + k * Q + j]);
+            for (int k = 0; k < R; ++k) cr.c2[kchunk<kChunkLog, Q>(k)][sj ^ koff<kChunkLog, Q>(k)] = lkmul(lcfold(x[k]), tab2[toff + k * Q + j]);
         }
         {
             F1 x[R];
@@ -148,7 +166,7 @@ __device__ __noinline__ void cl_dif_first(const uint32_t* __restrict__ lim, int 
             for (int k = 0; k < R; ++k) x[k] = real_times<F1>(v[k], tab1[coff + k]);
             bf_dif<R, F1>(x);
 #pragma unroll
-            for (int k = 0; k < R; ++k) ch.template e1<kChunkLog>(j + k * Q) = cmul(x[k], tab1[toff + k * Q + j]);
+            for (int k = 0; k < R; ++k) cr.c1[kchunk<kChunkLog, Q>(k)][sj ^ koff<kChunkLog, Q>(k)] = cmul(x[k], tab1[toff + k * Q + j]);
         }
     }
     cl.sync();
@@ -161,28 +179,31 @@ __device__ __noinline__ void cl_dit_last(const Chunks<C>& ch, const F2K* tab2, c
     constexpr int toff = tab_inv_off(M, 0, true), coff = tab_out_const_off(M, true);
     cl.sync();   // the local passes before this one wrote every chunk
     const int j0 = (int)cl.block_rank() * QC;
+    const ChunkRegs<C> cr(ch);
+    static_assert((1 << kChunkLog) % Q == 0, "the passes' spans divide the chunk length");
 #pragma unroll 1
     for (int j = j0 + (int)threadIdx.x; j < j0 + QC; j += NT) {
+        const int sj = swz(j);
         {
             F2 x[R];
 #pragma unroll
-            for (int k = 0; k < R; ++k) x[k] = lkmul(ch.template e2<kChunkLog>(j + k * Q), tab2[toff + k * Q + j]);
+            for (int k = 0; k < R; ++k) x[k] = lkmul(cr.c2[kchunk<kChunkLog, Q>(k)][sj ^ koff<kChunkLog, Q>(k)], tab2[toff + k * Q + j]);
             ldit<R>(x);
 #pragma unroll
             for (int k = 0; k < R; ++k) {
-                if (REAL_ONLY) ch.template e2<kChunkLog>(j + k * Q).re = lkmul_re(x[k], tab2[coff + k]);
-                else ch.template e2<kChunkLog>(j + k * Q) = lkmul(x[k], tab2[coff + k]);
+                if (REAL_ONLY) cr.c2[kchunk<kChunkLog, Q>(k)][sj ^ koff<kChunkLog, Q>(k)].re = lkmul_re(x[k], tab2[coff + k]);
+                else cr.c2[kchunk<kChunkLog, Q>(k)][sj ^ koff<kChunkLog, Q>(k)] = lkmul(x[k], tab2[coff + k]);
             }
         }
         {
             F1 x[R];
 #pragma unroll
-            for (int k = 0; k < R; ++k) x[k] = cmul(ch.template e1<kChunkLog>(j + k * Q), tab1[toff + k * Q + j]);
+            for (int k = 0; k < R; ++k) x[k] = cmul(cr.c1[kchunk<kChunkLog, Q>(k)][sj ^ koff<kChunkLog, Q>(k)], tab1[toff + k * Q + j]);
             bf_dit<R, F1>(x);
 #pragma unroll
             for (int k = 0; k < R; ++k) {
-                if (REAL_ONLY) ch.template e1<kChunkLog>(j + k * Q).re = cmul_re(x[k], tab1[coff + k]);
-                else ch.template e1<kChunkLog>(j + k * Q) = cmul(x[k], tab1[coff + k]);
+                if (REAL_ONLY) cr.c1[kchunk<kChunkLog, Q>(k)][sj ^ koff<kChunkLog, Q>(k)].re = cmul_re(x[k], tab1[coff + k]);
+                else cr.c1[kchunk<kChunkLog, Q>(k)][sj ^ koff<kChunkLog, Q>(k)] = cmul(x[k], tab1[coff + k]);
             }
         }
     }
@@ -198,12 +219,15 @@ __device__ __noinline__ void cl_half_pass0(const Chunks<C>& ch, const F2K* ht2, 
     static_assert(Q > 1, "the half transform has more than one pass");
     if (!FWD) cl.sync();
     const int j0 = (int)cl.block_rank() * QC;
+    const ChunkRegs<C> cr(ch);
+    static_assert((1 << LOG) % Q == 0, "the passes' spans divide the chunk length");
 #pragma unroll 1
     for (int j = j0 + (int)threadIdx.x; j < j0 + QC; j += NT) {
+        const int sj = swz(j);
         {
             F2 x[R];
 #pragma unroll
-            for (int k = 0; k < R; ++k) x[k] = ch.template e2<LOG>(j + k * Q);
+            for (int k = 0; k < R; ++k) x[k] = cr.c2[kchunk<LOG, Q>(k)][sj ^ koff<LOG, Q>(k)];
             if (FWD) {
                 ldif<R>(x);
                 x[0] = lcfold(x[0]);
@@ -215,12 +239,12 @@ __device__ __noinline__ void cl_half_pass0(const Chunks<C>& ch, const F2K* ht2, 
                 ldit<R>(x);
             }
 #pragma unroll
-            for (int k = 0; k < R; ++k) ch.template e2<LOG>(j + k * Q) = x[k];
+            for (int k = 0; k < R; ++k) cr.c2[kchunk<LOG, Q>(k)][sj ^ koff<LOG, Q>(k)] = x[k];
         }
         {
             F1 x[R];
 #pragma unroll
-            for (int k = 0; k < R; ++k) x[k] = ch.template e1<LOG>(j + k * Q);
+            for (int k = 0; k < R; ++k) x[k] = cr.c1[kchunk<LOG, Q>(k)][sj ^ koff<LOG, Q>(k)];
             if (FWD) {
                 bf_dif<R, F1>(x);
 #pragma unroll
@@ -231,7 +255,7 @@ __device__ __noinline__ void cl_half_pass0(const Chunks<C>& ch, const F2K* ht2, 
                 bf_dit<R, F1>(x);
             }
 #pragma unroll
-            for (int k = 0; k < R; ++k) ch.template e1<LOG>(j + k * Q) = x[k];
+            for (int k = 0; k < R; ++k) cr.c1[kchunk<LOG, Q>(k)][sj ^ koff<LOG, Q>(k)] = x[k];
         }
     }
     cl.sync();
@@ -352,12 +376,16 @@ __device__ __noinline__ uint64_t cl_carry_product(const Chunks<C>& ch, uint32_t*
     const int q0 = (int)cl.block_rank() * (2 * N / C) + (int)threadIdx.x * E;
     const bool hi = q0 >= N;
     const int j0 = hi ? q0 - N : q0;
+    // The run [j0, j0 + E) lies in one chunk (E divides the chunk length).
+    const F2* b2 = ch.c2[j0 >> kChunkLog];
+    const F1* b1 = ch.c1[j0 >> kChunkLog];
+    const int sb = swz(j0 & (kChunk - 1));
     uint32_t L[E];
     Acc96 acc;
 #pragma unroll
     for (int e = 0; e < E; ++e) {
-        const F2 a2 = ch.template e2<kChunkLog>(j0 + e);
-        const F1 a1 = ch.template e1<kChunkLog>(j0 + e);
+        const F2 a2 = b2[sb ^ swz_c(e)];
+        const F1 a1 = b1[sb ^ swz_c(e)];
         uint32_t w0, w1, w2;
         crt3(hi ? a1.im : a1.re, hi ? a2.im : a2.re, w0, w1, w2);
         L[e] = acc.add_shift(w0, w1, w2);
@@ -381,18 +409,18 @@ __device__ __noinline__ void cl_carry_low_and_pack(F2* s2, F1* s1, uint64_t* sc,
 #pragma unroll
     for (int e = 0; e < E; ++e) {
         uint32_t w0, w1, w2;
-        crt3(s1[swz(l0 + e)].re, s2[swz(l0 + e)].re, w0, w1, w2);
+        crt3(s1[(swz(l0) ^ swz_c(e))].re, s2[(swz(l0) ^ swz_c(e))].re, w0, w1, w2);
         L[e] = acc.add_shift(w0, w1, w2);
     }
     cluster_resolve<E, NT, C>(L, acc.rest(), 0, sc, cc, cl);   // the carry out of the top is dropped (mod R)
 #pragma unroll
     for (int e = 0; e < E; e += 2) {
-        const int j = (l0 + e) >> 1;
+        const int sj = swz(l0 >> 1) ^ swz_c(e >> 1);   // (l0 + e) / 2, l0 / 2 a multiple of E / 2
         F2 z2; z2.re = L[e]; z2.im = L[e + 1];
         const uint32_t r0 = (L[e] & P1) + (L[e] >> 31), r1 = (L[e + 1] & P1) + (L[e + 1] >> 31);
         F1 z1; z1.re = min(r0, r0 - P1); z1.im = min(r1, r1 - P1);
-        s2[swz(j)] = z2;
-        s1[swz(j)] = z1;
+        s2[sj] = z2;
+        s1[sj] = z1;
     }
     cl.sync();
 }
@@ -410,9 +438,9 @@ __device__ __noinline__ bool cl_wrap_combine(const F2* s2, const F1* s1, const u
     Acc96 acc;
 #pragma unroll
     for (int e = 0; e < E; e += 2) {
-        const int j = (l0 + e) >> 1;
-        const F2 a2 = s2[swz(j)];
-        const F1 a1 = s1[swz(j)];
+        const int sj = swz(l0 >> 1) ^ swz_c(e >> 1);   // (l0 + e) / 2, l0 / 2 a multiple of E / 2
+        const F2 a2 = s2[sj];
+        const F1 a1 = s1[sj];
         uint32_t w0, w1, w2;
         crt3(a1.re, a2.re, w0, w1, w2);
         uint64_t lo = (((uint64_t)w1 << 32) | w0) + tl[q0 + e];

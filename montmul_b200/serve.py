@@ -3,19 +3,22 @@
 
 Requests arrive as a Poisson process. Each transform length has a lane: uniform batches
 ("segments") whose slots keep their Montgomery state and exponent on the device. A request is
-admitted as soon as a slot of its length is free; a lane grows by one segment while the device
-memory budget allows (admission by the per-slot bytes of its length), else the request waits.
-Every tick is one mixed-length plan launch over a work list of every busy slot (persistent blocks
-over device work queues, replayed from a CUDA graph; L = 16384 slots take a whole block, the
-others one of its two workers). The slowest length runs `quantum` steps and every other length
-the steps that take as long on its worker (from the tuned cost per step); when busy slots
-outnumber the workers, the budgets come in two sizes that pack the workers evenly.
-Then the slots that finished are read back and refilled in place with waiting requests: the
-batch is never drained.
+admitted as soon as a slot of its length is free in a segment with no launch in flight; a lane
+grows by one segment, while the device memory budget allows, only when no segment of it has room.
+Finished slots are read back and refilled in place with waiting requests: no batch is drained.
+
+Three launch policies run the segments:
+  stream (default)  each segment cycles on its own CUDA stream: one item-list launch of its
+                    length's uniform step kernel over its busy slots, each budgeted `slice_ms` of
+                    device time at its length's full-GPU rate; when the launch is done the host
+                    reads, refills and launches again, while the other segments keep running;
+  items             ticks: every busy segment's item-list launch, then a wait for all of them;
+  plan              ticks of one mixed-length persistent launch over a work list of every busy
+                    slot (the slowest length runs `quantum` steps, the others as long).
 
 A Fermat request loads 1, sets the exponent N - 1 and reports the verdict x == 1; a mul request
 (a b mod N) takes two slots of the same modulus and one mul launch. Each request's time to
-verdict runs from its arrival to the tick that read its result.
+verdict runs from its arrival to the read-back of its result.
 
     python -m montmul_b200 serve [--load 0.7 0.95] [--duration 40] [--lo 10000] [--hi 200000]
 """
@@ -137,11 +140,11 @@ class Segment:
 
 
 class Server:
-    """Lanes of segments per transform length, one plan over every segment."""
+    """Lanes of segments per transform length, run by one of the three launch policies."""
 
     def __init__(self, dev, base: int = 3, quantum: int = 128, segment_slots: int = 0, budget_frac: float = 0.5,
                  tuned: bool = True, checker: Optional["VerdictChecker"] = None, launch: str = "stream",
-                 slice_ms: float = 30.0):
+                 slice_ms: float = 120.0):
         from .backend import lib
         self.dev = dev
         self.lib = lib()
