@@ -185,8 +185,10 @@ void mm_b200_t_free(mm_b200_tbuf *b);
  * launch of run (0: the device default). step_ns: the measured time of one slot-step at full
  * occupancy, which orders the items of a mixed launch (0: a model of the transform work).
  * threads: threads per block of the shared-memory step kernel (0: the length's default; L = 4096,
- * 8192 and 16384 also build one alternative shape); get_schedule reports the shape in use. The
- * autotuner (montmul_b200.tune) measures these per length and caches them. */
+ * 8192 and 16384 also build one alternative shape); in cluster mode, threads per SM (0 or 512:
+ * one 512-thread block of 8192 elements per SM; 1024 at L = 32768: two 512-thread blocks of 4096
+ * elements per SM, a cluster of 4). get_schedule reports the shape in use. The autotuner
+ * (montmul_b200.tune) measures these per length and caches them. */
 typedef struct {
     int global;
     int launch_steps;

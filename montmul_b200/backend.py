@@ -363,7 +363,9 @@ class B200:
     def set_schedule(self, st, global_mode, launch_steps: int = 0, step_ns: float = 0.0, threads: int = 0):
         """global_mode: 0 (or False) shared memory, 1 (or True) global mode, 2 cluster mode
         (L = 32768 and 65536: one thread-block cluster per slot, the vector in the cluster's
-        shared memory). threads: threads per block of the shared-memory step (0: the default)."""
+        shared memory). threads: threads per block of the shared-memory step (0: the default); in
+        cluster mode, threads per SM (0 or 512: one block of 8,192 elements per SM; 1024 at
+        L = 32768: two blocks of 4,096 elements per SM)."""
         sc = Schedule(int(global_mode), int(launch_steps), float(step_ns), int(threads))
         _check(lib().mm_b200_set_schedule(st.ptr, C.byref(sc)))
 

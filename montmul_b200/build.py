@@ -62,7 +62,8 @@ def build(force: bool = False, jobs: int | None = None, verbose: bool = False) -
         objs.append(obj)
         if force or _stale(obj, [src] + heads):
             jobs_list.append(([nv, *ARCH, *FLAGS, f"-DMM_M={m}", "-c", src, "-o", obj], obj, obj + ".log"))
-    for name in ("mm_backend", "mm_global", "mm_cluster", "mm_mixed", "mm_transform", "mm_peak", "mm_noalloc"):
+    for name in ("mm_backend", "mm_global", "mm_cluster", "mm_cluster_half", "mm_mixed", "mm_transform", "mm_peak",
+                 "mm_noalloc"):
         obj = os.path.join(BUILD, f"{name}.o")
         src = os.path.join(CSRC, f"{name}.cu")
         objs.append(obj)

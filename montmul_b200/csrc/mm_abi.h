@@ -64,13 +64,16 @@ struct GlobalKernels {
 };
 constexpr int kMinGlobalLogN = 12;   // smallest length the global kernels accept (one tile per half)
 GlobalKernels global_kernels();       // mm_global.cu
-// Cluster mode (mm_cluster.cu): L = 32768 and 65536, one thread-block cluster of n / 8192
-// blocks per slot. cluster_configure sets the kernels' shared-memory opt-in on the current
-// device; cluster_launch runs `bits` steps on every slot of a batch.
+// Cluster mode (mm_cluster.cu): L = 32768 and 65536, one thread-block cluster of n / 2^chunk_log
+// blocks per slot, 2^chunk_log elements in each: chunk_log 13 (one block per SM) at both
+// lengths, or 12 (two blocks per SM) at L = 32768. cluster_configure sets the kernels' shared-
+// memory opt-in on the current device; cluster_launch runs `bits` steps on every slot of a batch.
 constexpr int kMinClusterLogN = 14;
 constexpr int kMaxClusterLogN = 15;
+constexpr int kClusterChunkLog = 13;        // the default chunk
+constexpr int kClusterPairChunkLog = 12;    // the two-blocks-per-SM chunk, at L = 32768
 int cluster_configure();
-int cluster_launch(int m, const SlotArgs& a, uint32_t slots, uint32_t bits, void* stream);
+int cluster_launch(int m, int chunk_log, const SlotArgs& a, uint32_t slots, uint32_t bits, void* stream);
 // Enqueues wait_check_kernel (mm_global.cuh) on a stream; non-zero if the launch failed.
 int launch_wait_check(uint32_t* err, uint64_t limit_ns, void* stream);   // mm_global.cu
 

@@ -92,6 +92,7 @@ struct mm_b200_batch {
     int step_threads = 0;
     bool global = false;       // vector in HBM, tiles through shared memory (mm_global.cuh)
     bool cluster = false;      // global batch stepped in cluster mode (mm_cluster.cuh)
+    int cluster_chunk_log = kClusterChunkLog;   // elements per block of the cluster: 2^13 or 2^12
     const DevTables* ctab = nullptr;   // shared-layout tables of a cluster-mode length
     bool plain = false;        // REDC without the wraparound path (k may be below L/2)
     GlobalKernels gk{};
@@ -299,7 +300,7 @@ int launch_steps(mm_b200_batch* b, size_t bits, bool bare = false) {
             SlotArgs c = a;
             c.tab2 = b->ctab->t2;
             c.tab1 = b->ctab->t1;
-            const int e = cluster_launch(b->m, c, (uint32_t)b->slots, s, b->stream);
+            const int e = cluster_launch(b->m, b->cluster_chunk_log, c, (uint32_t)b->slots, s, b->stream);
             if (e) return fail(MM_ERR_CUDA, std::string("cluster launch: ") + cudaGetErrorString((cudaError_t)e));
         } else if (b->global) {
             b->gk.step<<<(unsigned)b->slots, b->gk.threads, b->gk.smem, b->stream>>>(g, 0, s);
@@ -865,6 +866,15 @@ int mm_b200_set_schedule(mm_b200_batch* b, const mm_b200_schedule* sc) {
     if (cluster && (b->m < kMinClusterLogN || b->m > kMaxClusterLogN))
         return fail(MM_ERR_UNSUPPORTED, "set_schedule: cluster mode runs L = 32768 and 65536 only");
     if (cluster && b->plain) return fail(MM_ERR_UNSUPPORTED, "set_schedule: cluster mode needs the wraparound path");
+    // Cluster mode: threads per SM picks the chunk, 512 (one 8,192-element block) or, at
+    // L = 32768, 1024 (two 4,096-element blocks of 512 threads).
+    int chunk_log = kClusterChunkLog;
+    if (cluster && sc->threads != 0 && sc->threads != 512) {
+        if (sc->threads != 1024 || b->m != kMinClusterLogN)
+            return fail(MM_ERR_UNSUPPORTED, "set_schedule: cluster mode runs 512 threads per SM"
+                                            " (1024 at L = 32768: two blocks per SM)");
+        chunk_log = kClusterPairChunkLog;
+    }
     StepFn fn = b->ks.step;
     int threads = b->ks.threads;
     if (!global && sc->threads != 0 && sc->threads != b->ks.threads) {
@@ -886,13 +896,14 @@ int mm_b200_set_schedule(mm_b200_batch* b, const mm_b200_schedule* sc) {
     }
     b->global = global;
     b->cluster = cluster;
+    b->cluster_chunk_log = chunk_log;
     if (!global) {
         b->step_fn = fn;
         b->step_threads = threads;
     }
     b->sched = *sc;
     b->sched.global = cluster ? 2 : (global ? 1 : 0);
-    b->sched.threads = global ? (cluster ? 512 : b->gk.threads) : threads;
+    b->sched.threads = global ? (cluster ? (chunk_log == kClusterChunkLog ? 512 : 1024) : b->gk.threads) : threads;
     return MM_OK;
 }
 

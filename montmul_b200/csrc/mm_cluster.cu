@@ -1,48 +1,30 @@
-// Kernel instantiations of cluster mode (L = 32768 and 65536) and their launch.
+// Kernel instantiations of cluster mode with 8,192-element chunks (L = 32768 and 65536) and the
+// launch of every cluster kernel. The 4,096-element-chunk kernel (L = 32768, two blocks per SM,
+// 64 registers) lives in mm_cluster_half.cu: its non-inlined passes are compiled there for 64
+// registers, leaving these kernels' copies their 128.
 #include "mm_cluster.cuh"
 
 namespace mm {
 
-namespace {
-
-template <int M>
-cudaError_t launch_cluster_m(const SlotArgs& a, uint32_t slots, uint32_t bits, cudaStream_t s) {
-    constexpr int C = 1 << (M - kChunkLog);
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(C * slots, 1, 1);
-    cfg.blockDim = dim3(kClusterThreads, 1, 1);
-    cfg.dynamicSmemBytes = kClusterSmem;
-    cfg.stream = s;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = C;
-    attr[0].val.clusterDim.y = 1;
-    attr[0].val.clusterDim.z = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, cluster_step_kernel<M>, a, 0u, bits);
-}
-
-template <int M>
-cudaError_t configure_cluster_m() {
-    return cudaFuncSetAttribute((const void*)cluster_step_kernel<M>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                kClusterSmem);
-}
-
-}  // namespace
 
 static_assert(kMaxClusterLogN - kChunkLog <= 3, "clusters of at most 8 blocks");
+static_assert(kClusterPairChunkLog == kChunkLog - 1, "the second chunk size is the default's half");
 
 int cluster_configure() {
-    cudaError_t e = configure_cluster_m<14>();
-    if (e == cudaSuccess) e = configure_cluster_m<15>();
+    cudaError_t e = configure_cluster_m<14, kChunkLog>();
+    if (e == cudaSuccess) e = configure_cluster_m<15, kChunkLog>();
+    if (e == cudaSuccess) e = cluster_half_chunk_configure();
     return (int)e;
 }
 
-int cluster_launch(int m, const SlotArgs& a, uint32_t slots, uint32_t bits, void* stream) {
+int cluster_launch(int m, int chunk_log, const SlotArgs& a, uint32_t slots, uint32_t bits, void* stream) {
     const cudaStream_t s = static_cast<cudaStream_t>(stream);
-    if (m == 14) return (int)launch_cluster_m<14>(a, slots, bits, s);
-    if (m == 15) return (int)launch_cluster_m<15>(a, slots, bits, s);
+    if (chunk_log == kChunkLog) {
+        if (m == 14) return (int)launch_cluster_m<14, kChunkLog>(a, slots, bits, s);
+        if (m == 15) return (int)launch_cluster_m<15, kChunkLog>(a, slots, bits, s);
+    } else if (chunk_log == kClusterPairChunkLog && m == 14) {
+        return (int)cluster_half_chunk_launch(a, slots, bits, s);
+    }
     return (int)cudaErrorInvalidValue;
 }
 

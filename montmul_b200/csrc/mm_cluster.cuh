@@ -23,7 +23,7 @@ namespace mm {
 
 namespace cgx = cooperative_groups;
 
-constexpr int kChunkLog = 13;                  // elements per CTA: 2^13
+constexpr int kChunkLog = kClusterChunkLog;     // elements per CTA by default: 2^13
 constexpr int kChunk = 1 << kChunkLog;
 constexpr int kClusterThreads = 512;
 constexpr int kClusterSmem = 24 * kChunk;      // 192 KiB
@@ -138,14 +138,14 @@ __device__ __forceinline__ uint64_t cluster_resolve(uint32_t (&L)[E], uint64_t c
 template <int M, int NT, int C>
 __device__ __noinline__ void cl_dif_first(const uint32_t* __restrict__ lim, int cnt, const Chunks<C>& ch, const F2K* tab2,
                                           const F1* tab1, const cgx::cluster_group& cl) {
-    constexpr int R = sched_radix(M, 0), Q = (1 << M) / R, QC = Q / C;
+    constexpr int R = sched_radix(M, 0), Q = (1 << M) / R, QC = Q / C, CL = M - ilog2c(C);
     constexpr int toff = tab_fwd_off(M, 0, true), coff = tab_in_const_off(M, true);
     // Every CTA has started, the limbs other CTAs wrote (x, T) are visible, and no CTA still
     // reads the chunks this pass overwrites.
     cl.sync();
     const int j0 = (int)cl.block_rank() * QC;
     const ChunkRegs<C> cr(ch);
-    static_assert((1 << kChunkLog) % Q == 0, "the passes' spans divide the chunk length");
+    static_assert((1 << CL) % Q == 0, "the passes' spans divide the chunk length");
 #pragma unroll 1
     for (int j = j0 + (int)threadIdx.x; j < j0 + QC; j += NT) {
         const int sj = swz(j);
@@ -158,7 +158,7 @@ __device__ __noinline__ void cl_dif_first(const uint32_t* __restrict__ lim, int 
             for (int k = 0; k < R; ++k) x[k] = lreal_times(v[k], tab2[coff + k]);
             ldif<R>(x);
 #pragma unroll
-            for (int k = 0; k < R; ++k) cr.c2[kchunk<kChunkLog, Q>(k)][sj ^ koff<kChunkLog, Q>(k)] = lkmul(lcfold(x[k]), tab2[toff + k * Q + j]);
+            for (int k = 0; k < R; ++k) cr.c2[kchunk<CL, Q>(k)][sj ^ koff<CL, Q>(k)] = lkmul(lcfold(x[k]), tab2[toff + k * Q + j]);
         }
         {
             F1 x[R];
@@ -166,7 +166,7 @@ __device__ __noinline__ void cl_dif_first(const uint32_t* __restrict__ lim, int 
             for (int k = 0; k < R; ++k) x[k] = real_times<F1>(v[k], tab1[coff + k]);
             bf_dif<R, F1>(x);
 #pragma unroll
-            for (int k = 0; k < R; ++k) cr.c1[kchunk<kChunkLog, Q>(k)][sj ^ koff<kChunkLog, Q>(k)] = cmul(x[k], tab1[toff + k * Q + j]);
+            for (int k = 0; k < R; ++k) cr.c1[kchunk<CL, Q>(k)][sj ^ koff<CL, Q>(k)] = cmul(x[k], tab1[toff + k * Q + j]);
         }
     }
     cl.sync();
@@ -175,35 +175,35 @@ __device__ __noinline__ void cl_dif_first(const uint32_t* __restrict__ lim, int 
 // The weighted last DIT pass (as dit_last_weighted), into natural order across the chunks.
 template <int M, int NT, int C, bool REAL_ONLY>
 __device__ __noinline__ void cl_dit_last(const Chunks<C>& ch, const F2K* tab2, const F1* tab1, const cgx::cluster_group& cl) {
-    constexpr int R = sched_radix(M, 0), Q = (1 << M) / R, QC = Q / C;
+    constexpr int R = sched_radix(M, 0), Q = (1 << M) / R, QC = Q / C, CL = M - ilog2c(C);
     constexpr int toff = tab_inv_off(M, 0, true), coff = tab_out_const_off(M, true);
     cl.sync();   // the local passes before this one wrote every chunk
     const int j0 = (int)cl.block_rank() * QC;
     const ChunkRegs<C> cr(ch);
-    static_assert((1 << kChunkLog) % Q == 0, "the passes' spans divide the chunk length");
+    static_assert((1 << CL) % Q == 0, "the passes' spans divide the chunk length");
 #pragma unroll 1
     for (int j = j0 + (int)threadIdx.x; j < j0 + QC; j += NT) {
         const int sj = swz(j);
         {
             F2 x[R];
 #pragma unroll
-            for (int k = 0; k < R; ++k) x[k] = lkmul(cr.c2[kchunk<kChunkLog, Q>(k)][sj ^ koff<kChunkLog, Q>(k)], tab2[toff + k * Q + j]);
+            for (int k = 0; k < R; ++k) x[k] = lkmul(cr.c2[kchunk<CL, Q>(k)][sj ^ koff<CL, Q>(k)], tab2[toff + k * Q + j]);
             ldit<R>(x);
 #pragma unroll
             for (int k = 0; k < R; ++k) {
-                if (REAL_ONLY) cr.c2[kchunk<kChunkLog, Q>(k)][sj ^ koff<kChunkLog, Q>(k)].re = lkmul_re(x[k], tab2[coff + k]);
-                else cr.c2[kchunk<kChunkLog, Q>(k)][sj ^ koff<kChunkLog, Q>(k)] = lkmul(x[k], tab2[coff + k]);
+                if (REAL_ONLY) cr.c2[kchunk<CL, Q>(k)][sj ^ koff<CL, Q>(k)].re = lkmul_re(x[k], tab2[coff + k]);
+                else cr.c2[kchunk<CL, Q>(k)][sj ^ koff<CL, Q>(k)] = lkmul(x[k], tab2[coff + k]);
             }
         }
         {
             F1 x[R];
 #pragma unroll
-            for (int k = 0; k < R; ++k) x[k] = cmul(cr.c1[kchunk<kChunkLog, Q>(k)][sj ^ koff<kChunkLog, Q>(k)], tab1[toff + k * Q + j]);
+            for (int k = 0; k < R; ++k) x[k] = cmul(cr.c1[kchunk<CL, Q>(k)][sj ^ koff<CL, Q>(k)], tab1[toff + k * Q + j]);
             bf_dit<R, F1>(x);
 #pragma unroll
             for (int k = 0; k < R; ++k) {
-                if (REAL_ONLY) cr.c1[kchunk<kChunkLog, Q>(k)][sj ^ koff<kChunkLog, Q>(k)].re = cmul_re(x[k], tab1[coff + k]);
-                else cr.c1[kchunk<kChunkLog, Q>(k)][sj ^ koff<kChunkLog, Q>(k)] = cmul(x[k], tab1[coff + k]);
+                if (REAL_ONLY) cr.c1[kchunk<CL, Q>(k)][sj ^ koff<CL, Q>(k)].re = cmul_re(x[k], tab1[coff + k]);
+                else cr.c1[kchunk<CL, Q>(k)][sj ^ koff<CL, Q>(k)] = cmul(x[k], tab1[coff + k]);
             }
         }
     }
@@ -211,10 +211,10 @@ __device__ __noinline__ void cl_dit_last(const Chunks<C>& ch, const F2K* tab2, c
 }
 
 // The first (DIF) or last (DIT) pass of the unweighted half-length transform (length 2^MH over
-// chunks of 2^(kChunkLog - 1) elements per CTA), across CTAs.
+// chunks of 2^MH / C elements per CTA), across CTAs.
 template <int MH, bool FWD, int NT, int C>
 __device__ __noinline__ void cl_half_pass0(const Chunks<C>& ch, const F2K* ht2, const F1* ht1, const cgx::cluster_group& cl) {
-    constexpr int R = sched_radix(MH, 0), Q = (1 << MH) / R, QC = Q / C, LOG = kChunkLog - 1;
+    constexpr int R = sched_radix(MH, 0), Q = (1 << MH) / R, QC = Q / C, LOG = MH - ilog2c(C);
     constexpr int toff = FWD ? tab_fwd_off(MH, 0, false) : tab_inv_off(MH, 0, false);
     static_assert(Q > 1, "the half transform has more than one pass");
     if (!FWD) cl.sync();
@@ -265,7 +265,7 @@ __device__ __noinline__ void cl_half_pass0(const Chunks<C>& ch, const F2K* ht2, 
 template <int MH, int NT, int C>
 __device__ __noinline__ void cl_half_pointwise(const Chunks<C>& ch, const F2* __restrict__ ab2, const F1* __restrict__ ab1,
                                                const cgx::cluster_group& cl) {
-    constexpr int H = 1 << MH, PAIRS = H / 2 + 1, PC = (PAIRS + C - 1) / C, LOG = kChunkLog - 1;
+    constexpr int H = 1 << MH, PAIRS = H / 2 + 1, PC = (PAIRS + C - 1) / C, LOG = MH - ilog2c(C);
     cl.sync();
     const int r = (int)cl.block_rank();
     const int t1 = min(PAIRS, (r + 1) * PC);
@@ -306,18 +306,18 @@ __device__ __noinline__ void cl_half_pointwise(const Chunks<C>& ch, const F2* __
 // ---- local passes of a transform on the CTA's own chunk ----
 // Passes 1 .. P - 2 of the length-2^M weighted transform (DIF) or P - 2 .. 1 (DIT); each stays
 // inside 8,192 elements for these lengths.
-template <int M, int NT, bool FWD>
+template <int M, int NT, bool FWD, int CL>
 __device__ __forceinline__ void cl_local_full(F2* s2, F1* s1, const F2K* tab2, const F1* tab1) {
     constexpr int P = sched_passes(M);
-    static_assert(sched_radix(M, 1) * sched_q(M, 1) <= kChunk, "only the first pass may cross chunks");
+    static_assert(sched_radix(M, 1) * sched_q(M, 1) <= (1 << CL), "only the first pass may cross chunks");
     if (FWD) {
 #pragma unroll
         for (int i = 1; i < P - 1; ++i) {
             const int R = sched_radix(M, i);
             const F2K* t2 = tab2 + tab_fwd_off(M, i, true);
             const F1* t1 = tab1 + tab_fwd_off(M, i, true);
-            if (R == 8) pass_rt<8, true, NT, true>(s2, s1, t2, t1, ilog2c(sched_q(M, i)), kChunk / 8);
-            else pass_rt<4, true, NT, true>(s2, s1, t2, t1, ilog2c(sched_q(M, i)), kChunk / 4);
+            if (R == 8) pass_rt<8, true, NT, true>(s2, s1, t2, t1, ilog2c(sched_q(M, i)), (1 << CL) / 8);
+            else pass_rt<4, true, NT, true>(s2, s1, t2, t1, ilog2c(sched_q(M, i)), (1 << CL) / 4);
         }
     } else {
 #pragma unroll
@@ -325,17 +325,17 @@ __device__ __forceinline__ void cl_local_full(F2* s2, F1* s1, const F2K* tab2, c
             const int R = sched_radix(M, i);
             const F2K* t2 = tab2 + tab_inv_off(M, i, true);
             const F1* t1 = tab1 + tab_inv_off(M, i, true);
-            if (R == 8) pass_rt<8, false, NT, true>(s2, s1, t2, t1, ilog2c(sched_q(M, i)), kChunk / 8);
-            else pass_rt<4, false, NT, true>(s2, s1, t2, t1, ilog2c(sched_q(M, i)), kChunk / 4);
+            if (R == 8) pass_rt<8, false, NT, true>(s2, s1, t2, t1, ilog2c(sched_q(M, i)), (1 << CL) / 8);
+            else pass_rt<4, false, NT, true>(s2, s1, t2, t1, ilog2c(sched_q(M, i)), (1 << CL) / 4);
         }
     }
 }
 
 // Passes 1 .. P - 1 (DIF) or P - 1 .. 1 (DIT) of the unweighted half-length transform on the
-// CTA's chunk of 2^(kChunkLog - 1) elements.
-template <int MH, int NT, bool FWD>
+// CTA's chunk of 2^(CL - 1) elements.
+template <int MH, int NT, bool FWD, int CL>
 __device__ __forceinline__ void cl_local_half(F2* s2, F1* s1, const F2K* ht2, const F1* ht1) {
-    constexpr int P = sched_passes(MH), HC = kChunk / 2;
+    constexpr int P = sched_passes(MH), HC = (1 << CL) / 2;
     static_assert(sched_radix(MH, 1) * sched_q(MH, 1) <= HC, "only the first half pass may cross chunks");
     if (FWD) {
 #pragma unroll
@@ -368,18 +368,18 @@ __device__ __forceinline__ void cl_local_half(F2* s2, F1* s1, const F2K* ht2, co
 
 // ---- carries over the cluster ----
 // T = c x^2 (2n limbs to `out`): CTA r owns coefficients [r 2n / C, (r + 1) 2n / C) of the
-// chain, E = 2 kChunk / NT per thread; coefficient q < n is re of element q, q >= n im of q - n.
+// chain, E = 2 n / (C NT) per thread; coefficient q < n is re of element q, q >= n im of q - n.
 template <int M, int NT, int C>
 __device__ __noinline__ uint64_t cl_carry_product(const Chunks<C>& ch, uint32_t* __restrict__ out, uint64_t* sc,
                                                   ClusterCarry* cc, const cgx::cluster_group& cl) {
-    constexpr int N = 1 << M, E = 2 * kChunk / NT;
+    constexpr int N = 1 << M, CL = M - ilog2c(C), E = 2 * (1 << CL) / NT;
     const int q0 = (int)cl.block_rank() * (2 * N / C) + (int)threadIdx.x * E;
     const bool hi = q0 >= N;
     const int j0 = hi ? q0 - N : q0;
     // The run [j0, j0 + E) lies in one chunk (E divides the chunk length).
-    const F2* b2 = ch.c2[j0 >> kChunkLog];
-    const F1* b1 = ch.c1[j0 >> kChunkLog];
-    const int sb = swz(j0 & (kChunk - 1));
+    const F2* b2 = ch.c2[j0 >> CL];
+    const F1* b1 = ch.c1[j0 >> CL];
+    const int sb = swz(j0 & ((1 << CL) - 1));
     uint32_t L[E];
     Acc96 acc;
 #pragma unroll
@@ -397,12 +397,12 @@ __device__ __noinline__ uint64_t cl_carry_product(const Chunks<C>& ch, uint32_t*
 }
 
 // m = the low n limbs of the product (real parts), packed into the half vector as
-// z_j = m_2j + i m_2j+1: CTA r owns coefficients [r kChunk, (r + 1) kChunk), all in its own
+// z_j = m_2j + i m_2j+1: CTA r owns coefficients [r n / C, (r + 1) n / C), all in its own
 // chunk, and its packed elements are its own half-vector chunk.
 template <int M, int NT, int C>
 __device__ __noinline__ void cl_carry_low_and_pack(F2* s2, F1* s1, uint64_t* sc, ClusterCarry* cc,
                                                    const cgx::cluster_group& cl) {
-    constexpr int E = kChunk / NT;
+    constexpr int E = (1 << (M - ilog2c(C))) / NT;
     const int l0 = (int)threadIdx.x * E;   // local coefficient index
     uint32_t L[E];
     Acc96 acc;
@@ -426,14 +426,14 @@ __device__ __noinline__ void cl_carry_low_and_pack(F2* s2, F1* s1, uint64_t* sc,
 }
 
 // x = floor(T / R) + ((cyclic + T mod R) mod (R - 1)) as wrap_combine: CTA r owns limbs
-// [r kChunk, (r + 1) kChunk), the cyclic product's coefficients packed in its half chunk.
+// [r n / C, (r + 1) n / C), the cyclic product's coefficients packed in its half chunk.
 template <int M, int NT, int C>
 __device__ __noinline__ bool cl_wrap_combine(const F2* s2, const F1* s1, const uint32_t* __restrict__ tl,
                                              uint32_t* __restrict__ x, uint64_t* sc, ClusterCarry* cc,
                                              const cgx::cluster_group& cl) {
-    constexpr int K = 1 << M, E = kChunk / NT;
+    constexpr int K = 1 << M, CL = M - ilog2c(C), E = (1 << CL) / NT;
     const int l0 = (int)threadIdx.x * E;
-    const int q0 = (int)cl.block_rank() * kChunk + l0;
+    const int q0 = (int)cl.block_rank() * (1 << CL) + l0;
     uint32_t L[E];
     Acc96 acc;
 #pragma unroll
@@ -473,10 +473,11 @@ __device__ __noinline__ bool cl_wrap_combine(const F2* s2, const F1* s1, const u
 template <int M, int NT, int C>
 __device__ __forceinline__ void cl_step_slot(const SlotArgs& a, uint32_t slot, uint32_t bits, unsigned char* smem_raw,
                                              uint64_t* sc, ClusterCarry* cc) {
-    constexpr int N = 1 << M, MH = M - 1;
+    constexpr int N = 1 << M, MH = M - 1, CL = M - ilog2c(C), CH = 1 << CL;
+    static_assert(CH * C == N, "C chunks of 2^CL elements hold the vector");
     const cgx::cluster_group cl = cgx::this_cluster();
     F2* s2 = reinterpret_cast<F2*>(smem_raw);
-    F1* s1 = reinterpret_cast<F1*>(smem_raw + 16 * kChunk);
+    F1* s1 = reinterpret_cast<F1*>(smem_raw + 16 * CH);
     Chunks<C> ch;
 #pragma unroll
     for (int d = 0; d < C; ++d) {
@@ -493,32 +494,32 @@ __device__ __forceinline__ void cl_step_slot(const SlotArgs& a, uint32_t slot, u
     const F1* ht1 = a.tab1 + lt_half_off(M);
     const uint32_t nb = a.nbits[slot];
     uint32_t pos = a.pos[slot];
-    const int gbase = r * (kChunk / 8);   // this CTA's first group of the span-1 pass
+    const int gbase = r * (CH / 8);   // this CTA's first group of the span-1 pass
     bool ok = true;
     for (uint32_t it = 0; it < bits && pos < nb; ++it, ++pos) {
         const uint32_t bit = (ex[pos >> 5] >> (31 - (pos & 31))) & 1;
         const uint32_t c = bit ? a.base : 1;
         // T = c x^2
         cl_dif_first<M, NT, C>(x, N, ch, a.tab2, a.tab1, cl);
-        cl_local_full<M, NT, true>(s2, s1, a.tab2, a.tab1);
-        fused_mid<kChunkLog, NT, false>(nullptr, 0, s2, s1, a.tab2, a.tab1, TileOp<SquareOp>{SquareOp{c}, gbase});
-        cl_local_full<M, NT, false>(s2, s1, a.tab2, a.tab1);
+        cl_local_full<M, NT, true, CL>(s2, s1, a.tab2, a.tab1);
+        fused_mid<CL, NT, false>(nullptr, 0, s2, s1, a.tab2, a.tab1, TileOp<SquareOp>{SquareOp{c}, gbase});
+        cl_local_full<M, NT, false, CL>(s2, s1, a.tab2, a.tab1);
         cl_dit_last<M, NT, C, false>(ch, a.tab2, a.tab1, cl);
         ok &= cl_carry_product<M, NT, C>(ch, tl, sc, cc, cl) == 0;
         if (a.bare) continue;
         // m = (T mod R) N' mod R
         cl_dif_first<M, NT, C>(tl, N, ch, a.tab2, a.tab1, cl);
-        cl_local_full<M, NT, true>(s2, s1, a.tab2, a.tab1);
-        fused_mid<kChunkLog, NT, true>(nullptr, 0, s2, s1, a.tab2, a.tab1,
+        cl_local_full<M, NT, true, CL>(s2, s1, a.tab2, a.tab1);
+        fused_mid<CL, NT, true>(nullptr, 0, s2, s1, a.tab2, a.tab1,
                                        TileOp<SpecMulRT>{SpecMulRT{cc2, cc1, N / 8}, gbase});
-        cl_local_full<M, NT, false>(s2, s1, a.tab2, a.tab1);
+        cl_local_full<M, NT, false, CL>(s2, s1, a.tab2, a.tab1);
         cl_dit_last<M, NT, C, true>(ch, a.tab2, a.tab1, cl);
         cl_carry_low_and_pack<M, NT, C>(s2, s1, sc, cc, cl);
         // m N mod (R - 1) through the half-length transform of the packed limbs
         cl_half_pass0<MH, true, NT, C>(ch, ht2, ht1, cl);
-        cl_local_half<MH, NT, true>(s2, s1, ht2, ht1);
+        cl_local_half<MH, NT, true, CL>(s2, s1, ht2, ht1);
         cl_half_pointwise<MH, NT, C>(ch, cc2 + N, cc1 + N, cl);
-        cl_local_half<MH, NT, false>(s2, s1, ht2, ht1);
+        cl_local_half<MH, NT, false, CL>(s2, s1, ht2, ht1);
         cl_half_pass0<MH, false, NT, C>(ch, ht2, ht1, cl);
         ok &= cl_wrap_combine<M, NT, C>(s2, s1, tl, x, sc, cc, cl);
     }
@@ -529,14 +530,47 @@ __device__ __forceinline__ void cl_step_slot(const SlotArgs& a, uint32_t slot, u
     }
 }
 
-// The uniform cluster launch: cluster i (C consecutive blocks) steps slot first + i.
-template <int M>
-__global__ void __launch_bounds__(kClusterThreads, 1) cluster_step_kernel(SlotArgs a, uint32_t first, uint32_t bits) {
-    constexpr int C = 1 << (M - kChunkLog);
+// The uniform cluster launch: cluster i (C = 2^(M - CL) consecutive blocks of 2^CL elements)
+// steps slot first + i. CL = 13: one block of 192 KiB per SM; CL = 12 (L = 32768 only): two
+// blocks of 96 KiB per SM, so twice the warps hide the latency of the cross-block accesses, at
+// 64 registers per thread and with more of each cross-block pass remote.
+template <int M, int CL>
+__global__ void __launch_bounds__(kClusterThreads, kChunkLog - CL + 1)
+    cluster_step_kernel(SlotArgs a, uint32_t first, uint32_t bits) {
+    constexpr int C = 1 << (M - CL);
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ uint64_t sc[CarryScratch<kClusterThreads>::words];
     __shared__ ClusterCarry cc;
     cl_step_slot<M, kClusterThreads, C>(a, first + blockIdx.x / C, bits, smem_raw, sc, &cc);
 }
+
+// ---- host side: launch and shared-memory opt-in of one instantiation ----
+template <int M, int CL>
+cudaError_t launch_cluster_m(const SlotArgs& a, uint32_t slots, uint32_t bits, cudaStream_t s) {
+    constexpr int C = 1 << (M - CL);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(C * slots, 1, 1);
+    cfg.blockDim = dim3(kClusterThreads, 1, 1);
+    cfg.dynamicSmemBytes = 24 << CL;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = C;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, cluster_step_kernel<M, CL>, a, 0u, bits);
+}
+
+template <int M, int CL>
+cudaError_t configure_cluster_m() {
+    return cudaFuncSetAttribute((const void*)cluster_step_kernel<M, CL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                24 << CL);
+}
+
+// The 4,096-element-chunk instantiation at L = 32768 (mm_cluster_half.cu).
+cudaError_t cluster_half_chunk_configure();
+cudaError_t cluster_half_chunk_launch(const SlotArgs& a, uint32_t slots, uint32_t bits, cudaStream_t s);
 
 }  // namespace mm

@@ -27,14 +27,17 @@ def main(argv=None):
     dev = B200(max_launch_steps=a.steps)
     b = ModBatch(dev, moduli, 3)
     be, st = b.backend_and_state()
+    shape = 0
     if a.mode == "tuned":
         row = tune.schedule_for(dev.device_name(), b.params.len)
         mode = int(row["global"]) if row else None
+        shape = int(row.get("block_threads", 0)) if row else 0
     else:
         mode = {"shared": tune.SHARED, "global": tune.GLOBAL, "cluster": tune.CLUSTER}[a.mode]
     if mode is not None:
-        be.set_schedule(st, mode, a.steps, 0.0, 0)
-    print(f"L = {b.params.len}, mode {be.get_schedule(st)['mode']}, {a.steps} steps per launch")
+        be.set_schedule(st, mode, a.steps, 0.0, shape)
+    sc = be.get_schedule(st)
+    print(f"L = {b.params.len}, mode {sc['mode']}, {sc['threads']} threads, {a.steps} steps per launch")
     arm(b, exps)
     for i in range(a.launches):
         t = time.perf_counter()

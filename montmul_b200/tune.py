@@ -76,11 +76,13 @@ def mode_name(mode) -> str:
     return ("shared", "global", "cluster")[int(mode)]
 
 
-def fixed_parts(length: int, global_mode):
+def fixed_parts(length: int, global_mode, block_threads: int = 0):
     n = length // 2
     m = n.bit_length() - 1
     if int(global_mode) == CLUSTER:
-        return {"threads": 512, "blocks_per_sm": 1, "cluster": n // CLUSTER_CHUNK, "tile": None,
+        # 1024 threads per SM: two 512-thread blocks of half the default chunk on each SM
+        chunk = CLUSTER_CHUNK // 2 if block_threads == 1024 else CLUSTER_CHUNK
+        return {"threads": 512, "blocks_per_sm": CLUSTER_CHUNK // chunk, "cluster": n // chunk, "tile": None,
                 "radix": radix_schedule(m)}
     if global_mode:
         g = m - TILE.bit_length() + 1
@@ -90,10 +92,15 @@ def fixed_parts(length: int, global_mode):
     return {"threads": threads_for(m), "blocks_per_sm": per_sm, "tile": None, "radix": radix_schedule(m)}
 
 
-def alt_threads(length: int) -> int:
-    """The alternative block shape of the shared-memory step at this length (mm_abi.h
-    alt_threads_for), 0 when none is built."""
+def alt_threads(length: int, mode: int = SHARED) -> int:
+    """The alternative shape at this length, 0 when none is built: in shared mode the step
+    kernel's other block size (mm_abi.h alt_threads_for); in cluster mode at L = 32768, 1024
+    threads per SM (two blocks of 4,096 elements per SM instead of one of 8,192)."""
     m = (length // 2).bit_length() - 1
+    if int(mode) == CLUSTER:
+        return 1024 if m == 14 else 0
+    if int(mode) == GLOBAL:
+        return 0
     return {11: 256, 12: 256, 13: 1024}.get(m, 0)
 
 
@@ -108,7 +115,7 @@ def candidates(length: int):
         modes.append(CLUSTER)
     out = []
     for g in modes:
-        shapes = [0] + ([alt_threads(length)] if g == SHARED and alt_threads(length) else [])
+        shapes = [0] + ([alt_threads(length, g)] if alt_threads(length, g) else [])
         out += [(g, s, th) for th in shapes for s in LAUNCH_STEPS]
     return out
 
@@ -182,8 +189,8 @@ def tune_length(dev, length: int, budget_s: float = 4.0):
     out = dict(best)
     if len(ranked) > 1:
         out["runner_up"] = dict(ranked[1])
-    out.update(fixed_parts(length, best["global"]))
-    if best.get("block_threads"):
+    out.update(fixed_parts(length, best["global"], best.get("block_threads", 0)))
+    if best.get("block_threads") and int(best["global"]) == SHARED:
         out["threads"] = best["block_threads"]
     out["slots"] = slots
     out["steps"] = steps

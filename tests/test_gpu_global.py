@@ -124,10 +124,11 @@ def test_bounded_wait_runs_out_and_context_stays_usable(gpu, wrap, bits):
         assert b.read(i) == powm(5 + i, 1 << e.bit_length(), n) * powm(3, e, n) % n
 
 
-@pytest.mark.parametrize("length,steps", [(1 << 15, 10), (1 << 16, 6)])
-def test_cluster_mode_same_raw_as_oracle(gpu, wrap, length, steps):
-    """Cluster mode (one thread-block cluster of L / 16384 blocks per slot, the vector in the
-    cluster's shared memory) at the top of the bucket: raw limbs equal Cpu::with_wraparound."""
+@pytest.mark.parametrize("length,steps,per_sm", [(1 << 15, 10, 512), (1 << 15, 10, 1024), (1 << 16, 6, 512)])
+def test_cluster_mode_same_raw_as_oracle(gpu, wrap, length, steps, per_sm):
+    """Cluster mode (one thread-block cluster per slot, the vector in the cluster's shared memory:
+    blocks of 8,192 elements, one per SM, or at L = 32768 blocks of 4,096 elements, two per SM)
+    at the top of the bucket: raw limbs equal Cpu::with_wraparound."""
     dev = gpu()
 
     class Cluster:
@@ -136,8 +137,9 @@ def test_cluster_mode_same_raw_as_oracle(gpu, wrap, length, steps):
 
         def create(self, *a):
             st = dev.create(*a)
-            dev.set_schedule(st, 2, 0)
-            assert dev.get_schedule(st)["mode"] == "cluster"
+            dev.set_schedule(st, 2, 0, threads=per_sm)
+            sc = dev.get_schedule(st)
+            assert sc["mode"] == "cluster" and sc["threads"] == per_sm
             return st
 
     common.same_raw(lambda: Cluster(), wrap, 16 * length - 4, 3, steps)
@@ -151,19 +153,24 @@ def test_cluster_mode_equals_global_mode_and_pow_mod(gpu, bits):
     moduli = [common.rand_odd(rng, bits) for _ in range(5)]
     exps = [common.rand_exponent(rng, 30) for _ in range(5)]
     runs = []
-    for modes in ((1, 1), (2, 1), (2, 2)):
+    # (mode, threads per SM) before and after the switch; at L = 32768 also the two-blocks-per-SM
+    # cluster shape, switched to and from mid-run
+    plans = [((1, 0), (1, 0)), ((2, 0), (1, 0)), ((2, 0), (2, 0))]
+    if bits == 300_000:
+        plans += [((2, 1024), (2, 0)), ((2, 0), (2, 1024)), ((1, 0), (2, 1024))]
+    for first, then in plans:
         b = ModBatch(gpu(), moduli, 3)
         be, st = b.backend_and_state()
         b.load_all([2, 3, 4, 5, 6])
         b.set_exponents(exps)
-        be.set_schedule(st, modes[0], 7)
+        be.set_schedule(st, first[0], 7, threads=first[1])
         b.run(13)
-        be.set_schedule(st, modes[1], 7)
+        be.set_schedule(st, then[0], 7, threads=then[1])
         b.run(30)
         runs.append([b.read_raw(i) for i in range(5)])
         for i, (n, e) in enumerate(zip(moduli, exps)):
             assert b.read(i) == powm(2 + i, 1 << e.bit_length(), n) * powm(3, e, n) % n
-    assert runs[0] == runs[1] == runs[2]
+    assert all(r == runs[0] for r in runs)
     b = ModBatch(gpu(), moduli[:2], 3)
     be, st = b.backend_and_state()
     be.set_schedule(st, 2, 0)
@@ -179,3 +186,7 @@ def test_cluster_mode_rejects_other_lengths(gpu):
     be, st = b.backend_and_state()
     with pytest.raises(MontMulError, match="cluster mode runs L = 32768 and 65536 only"):
         be.set_schedule(st, 2, 0)
+    b = ModBatch(gpu(), [common.rand_odd(RandState(4), 1_000_000)], 3)
+    be, st = b.backend_and_state()
+    with pytest.raises(MontMulError, match="cluster mode runs 512 threads per SM"):
+        be.set_schedule(st, 2, 0, threads=1024)

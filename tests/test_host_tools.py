@@ -32,6 +32,10 @@ def test_tune_candidates_by_length():
     assert {c[0] for c in tune.candidates(131072)} == {G}
     assert tune.fixed_parts(1 << 20, True)["radix"]["global"] == tune.radix_schedule(19 - 11)
     assert tune.fixed_parts(32768, C)["cluster"] == 2 and tune.fixed_parts(65536, C)["cluster"] == 4
+    assert tune.fixed_parts(32768, C, 1024)["cluster"] == 4 and tune.fixed_parts(32768, C, 1024)["blocks_per_sm"] == 2
+    assert {th for g, _, th in tune.candidates(32768) if g == C} == {0, 1024}
+    assert {th for g, _, th in tune.candidates(65536) if g == C} == {0}
+    assert {th for g, _, th in tune.candidates(32768) if g == G} == {0}
     assert [tune.mode_name(m) for m in (S, G, C, False, True)] == ["shared", "global", "cluster", "shared", "global"]
 
 
