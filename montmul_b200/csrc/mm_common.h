@@ -13,6 +13,9 @@
 #define MM_HD __host__ __device__ __forceinline__
 #else
 #define MM_HD inline
+#ifndef __align__
+#define __align__(n) __attribute__((aligned(n)))   // host-only builds of this header
+#endif
 #endif
 
 namespace mm {
@@ -32,6 +35,23 @@ constexpr int kMinLogN = 2;   // L = 8
 
 // Dynamic shared memory of one block at length 2^(m+1): F2 vector (16 n B), F1 vector (8 n B).
 MM_HD constexpr int smem_bytes_host(int m) { return 24 << m; }
+
+// Position of element e in shared memory (and in global mode's work vectors): e with its low
+// four bits flipped by a linear function of bits 3-8,
+//   bit 0 ^= e3 ^ e6 ^ e8,  bit 1 ^= e4 ^ e6 ^ e7,  bit 2 ^= e5,  bit 3 ^= e4 ^ e5 ^ e6.
+// Chosen by simulating every shared-memory access pattern of the kernels (each radix-8 and
+// radix-4 pass of both transforms at every span; the carries' runs of 2 to 32 consecutive
+// elements per thread and their pair-packed reads and writes; 16-B F2 and 8-B F1 accesses; 32 to
+// 1,024 threads per slot): every warp access of n >= 64 elements takes the minimum number of
+// wavefronts (tests/test_swizzle.py). Flipping the low bits by bits 3-6 alone left the carries'
+// runs of 16 and 32 elements 2- and 4-way conflicted. swz is linear over XOR,
+// swz(a ^ b) = swz(a) ^ swz(b), and permutes each aligned run of 16 elements.
+MM_HD constexpr int swz_c(int e) {
+    const int h = e >> 3, u = (h >> 3) & 7;   // h: bits 3.., u: bits 6-8
+    const int lo = (h ^ ((u ^ (u << 1) ^ (u >> 2)) & 3)) & 7;
+    const int b3 = ((h >> 1) ^ (h >> 2) ^ (h >> 3)) & 1;
+    return e ^ lo ^ (b3 << 3);
+}
 
 // ---- pass schedule: radices, DIF order ----
 // m = log2 n. m = 3a -> [8]*a; m = 3a + 1 -> [4, 4, 8*(a-1)]; m = 3a + 2 -> [4, 8*a];

@@ -10,15 +10,7 @@
 // position ends with exactly the value the reference's radix-2 loops produce.
 //
 // Shared-memory layout: F2 array (16 B per element) then F1 array (8 B), element e stored at
-// swz(e): e with its low four bits flipped by a linear function of bits 3-8,
-//   bit 0 ^= e3 ^ e6 ^ e8,  bit 1 ^= e4 ^ e6 ^ e7,  bit 2 ^= e5,  bit 3 ^= e4 ^ e5 ^ e6.
-// Simulated over every shared-memory access pattern of the kernels (each radix-8 and radix-4 pass
-// of both transforms at every span; the carries' runs of 2 to 32 consecutive elements per
-// thread and their pair-packed reads and writes; 16-B F2 and 8-B F1 accesses; 32 to 1,024
-// threads per slot), every warp access of n >= 64 elements takes the minimum number of
-// wavefronts. (Flipping the low bits by bits 3-6 alone left the carries' runs of 16 and 32
-// elements 2- and 4-way conflicted.) swz is linear over XOR, swz(a ^ b) = swz(a) ^ swz(b), and
-// permutes each aligned run of 16 elements.
+// swz(e) (swz_c, mm_common.h): conflict-free for every pass and carry of the kernels.
 #pragma once
 #include "mm_field.cuh"
 
@@ -49,12 +41,6 @@ template <int NT> __device__ __forceinline__ int gsync_or(int pred) {
     return r;
 }
 
-MM_HD constexpr int swz_c(int e) {
-    const int h = e >> 3, u = (h >> 3) & 7;   // h: bits 3.., u: bits 6-8
-    const int lo = (h ^ ((u ^ (u << 1) ^ (u >> 2)) & 3)) & 7;
-    const int b3 = ((h >> 1) ^ (h >> 2) ^ (h >> 3)) & 1;
-    return e ^ lo ^ (b3 << 3);
-}
 __device__ __forceinline__ int swz(int e) { return swz_c(e); }
 
 // ---- in-register butterflies (positions k of one group) ----
